@@ -1,0 +1,403 @@
+"""Benchmark of the partitioned SpMM on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload fp32|bf16]
+
+Default workload: R-MAT scale 20 (1,048,576 nodes), avg degree 32, symmetrised,
+values D^-1/2 A D^-1/2, P = 8 virtual row partitions, X 1,048,576 x 128 FP32
+~N(0,1) (Philox, seed 2), FP32 output.  A step is one Y = A X over all
+partitions (Y zeroed, then one fused launch), inputs resident in HBM.  The
+metric is algorithmic HBM GB/s:
+    B = nnz*(4 + s_v + K*s_x) + (M+1)*4 + M*K*s_y   (s_v = 4)
+per step divided by the step time.  Inputs (X 512 MiB, Y 512 MiB) are larger
+than L2, so no L2 flush runs between timed steps.
+
+Multi-GPU (torchrun): every rank runs an independent replica of the workload
+on its own GPU (replicas only: the single-GPU path has no exchange between
+GPUs); value = all ranks' bytes / the slowest rank's time.
+
+--impl reference times the reference's own CPU SpMM (SAG_reference_host of
+include/utils.cuh, compiled from the reference tree into oracle/_ref) on the
+host cores, on a bounded row sample per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+WORKLOADS = {
+    # name: (scale, avg_degree, K, nparts, x dtype, y dtype, seed)
+    "fp32": dict(scale=20, deg=32, K=128, P=8, xdt="fp32", ydt="fp32", seed=2,
+                 desc="R-MAT scale 20 (1,048,576 nodes), avg degree 32, D^-1/2 A D^-1/2; X 1,048,576x128 FP32; "
+                      "P=8 virtual row partitions"),
+    "bf16": dict(scale=21, deg=48, K=256, P=8, xdt="bf16", ydt="bf16", seed=3,
+                 desc="R-MAT scale 21 (2,097,152 nodes), avg degree 48, D^-1/2 A D^-1/2; X 2,097,152x256 BF16 "
+                      "(from FP32 N(0,1)), FP32 accumulation, BF16 output; P=8 virtual row partitions"),
+}
+METRIC = "SpMM HBM GB/s (algorithmic bytes / step time)"
+
+
+def alg_bytes(nnz, M, K, s_x, s_y, s_v=4):
+    return nnz * (4 + s_v + K * s_x) + (M + 1) * 4 + M * K * s_y
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def make_graph(w):
+    import cola_b200 as cb
+    n, row, col, val = cb.rmat(w["scale"], w["deg"], w["seed"])
+    return n, row, col, val
+
+
+def dense_x(n, K, seed):
+    g = np.random.Generator(np.random.Philox(seed))
+    return g.standard_normal((n, K), dtype=np.float32)
+
+
+def read_traffic(name):
+    """traffic_bytes_per_launch from a committed ncu summary, if any."""
+    p = os.path.join(REPO, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.strip().startswith("traffic_bytes_per_launch"):
+                try:
+                    return int(float(line.split("=")[1].split()[0]))
+                except (IndexError, ValueError):
+                    return None
+    return None
+
+
+def measured_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own SAG_reference_host on host threads
+# ---------------------------------------------------------------------------
+def cpu_sample(rp, ci, X, K, nthreads, target_s, rows_hint=None):
+    """Runs the reference CPU SpMM over `nthreads` disjoint row blocks spread
+    over the matrix.  Returns (seconds, rows, nnz, kind)."""
+    from oracle import oracle
+    n = len(rp) - 1
+    kind = "reference" if oracle.ref_available() else "port"
+    rows_per = rows_hint or max(1, min(n // nthreads, 2048))
+    blocks = []
+    for t in range(nthreads):
+        lb = (n // nthreads) * t
+        ub = min(n, lb + rows_per)
+        blocks.append((lb, ub))
+    outs = [np.zeros(((ub - lb), K), np.float32) for lb, ub in blocks]
+    if kind == "reference":
+        R = oracle.ref()
+
+        def work(i):
+            lb, ub = blocks[i]
+            R.ref_sag_reference_host(lb, ub, K, rp.ctypes.data, ci.ctypes.data, X.ctypes.data,
+                                     outs[i].ctypes.data, 0)
+    else:
+        L = oracle.lib()
+
+        def work(i):
+            lb, ub = blocks[i]
+            Yd = np.zeros((ub - lb, K), np.float64)
+            sub = np.ascontiguousarray(rp[lb:ub + 1] - rp[lb], np.int32)
+            L.orc_spmm_csr_f64(ub - lb, sub.ctypes.data, ci[rp[lb]:].ctypes.data, None, X.ctypes.data, K, K,
+                               Yd.ctypes.data, K)
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=work, args=(i,)) for i in range(nthreads)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    dt = time.perf_counter() - t0
+    rows = sum(ub - lb for lb, ub in blocks)
+    nnz = int(sum(rp[ub] - rp[lb] for lb, ub in blocks))
+    return dt, rows, nnz, kind
+
+
+def calibrated_cpu(rp, ci, X, K, nthreads, target_s):
+    """Grow the per-thread row block until one sample takes ~target_s."""
+    n = len(rp) - 1
+    rows = 256
+    while True:
+        dt, r, nnz, kind = cpu_sample(rp, ci, X, K, nthreads, target_s, rows)
+        if dt >= target_s * 0.5 or rows >= n // nthreads:
+            return dt, r, nnz, kind, rows
+        rows = min(n // nthreads, int(rows * max(2.0, target_s / max(dt, 1e-3))))
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, w):
+    from oracle import oracle
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n, row, col, val = make_graph(w)
+    rp, ci, _ = oracle.global_csr(n, row, col, val)
+    K = w["K"]
+    X = dense_x(n, K, w["seed"])
+    nth = host_threads()
+    dt, rows, nnz, kind, rows_per = calibrated_cpu(rp, ci, X, K, nth, target_s=1.0)
+    for _ in range(max(args.warmup - 1, 0)):
+        cpu_sample(rp, ci, X, K, nth, 1.0, rows_per)
+    times = []
+    for _ in range(args.steps):
+        dt, rows, nnz, kind = cpu_sample(rp, ci, X, K, nth, 1.0, rows_per)[:4]
+        times.append(dt)
+    t = sum(times) / len(times)
+    s = 4 if w["xdt"] == "fp32" else 2
+    B = alg_bytes(nnz, rows, K, 4, 4)  # the reference computes in FP32
+    v = B / t / 1e9
+    sample = "{} threads x {} rows (rows spread over the matrix), {} of {} rows, {} nnz per step".format(
+        nth, rows_per, rows, n, nnz)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w["desc"], "nnz": len(row), "K": K, "parallelism": "host threads",
+                       "x_storage": w["xdt"] if s == 4 else "fp32 (reference has no BF16 path)"},
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": nth, "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, w):
+    import torch
+    import torch.distributed as dist
+
+    import cola_b200 as cb
+    from cola_b200 import spmm as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev)
+
+    t0 = time.time()
+    n, row, col, val = make_graph(w)
+    ps = cb.PartitionSet.from_coo(n, row, col, val, w["P"])
+    K = w["K"]
+    Xh = dense_x(n, K, w["seed"])
+    t_prep = time.time() - t0
+    stream = torch.cuda.current_stream()
+    g = S.Graph(ps, stream=stream)
+    info = g.info
+    xdt = torch.float32 if w["xdt"] == "fp32" else torch.bfloat16
+    ydt = torch.float32 if w["ydt"] == "fp32" else torch.bfloat16
+    s_x = 4 if xdt == torch.float32 else 2
+    s_y = 4 if ydt == torch.float32 else 2
+    X = torch.from_numpy(Xh).to(dev).to(xdt)
+    Y = torch.empty((n, K), dtype=ydt, device=dev)
+    sched = {"auto": S.SCHEDULE_AUTO, "fused": S.SCHEDULE_FUSED, "buffer": S.SCHEDULE_BUFFER}[args.schedule]
+    B = alg_bytes(int(info.nnz), n, K, s_x, s_y)
+
+    def step():
+        g.spmm(X, Y, schedule=sched, stream=stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    for _ in range(args.steps):
+        step()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    ms = max_over_ranks(ms)
+
+    # dominant kernel alone (accumulate mode: the same fused launch, no zeroing)
+    Yacc = torch.zeros((n, K), dtype=torch.float32, device=dev)
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for a, b in kev:
+        a.record(stream)
+        g.spmm(X, Yacc, accumulate=True, schedule=sched, stream=stream)
+        b.record(stream)
+    torch.cuda.synchronize()
+    k_ms = sum(a.elapsed_time(b) for a, b in kev) / len(kev)
+    k_ms = max_over_ranks(k_ms)
+    clk = clocks.stop()
+    del Yacc
+
+    # end to end through the public API: pinned host X -> device, SpMM, Y -> pinned host
+    Xpin = torch.from_numpy(Xh).to(xdt).pin_memory()
+    Ypin = torch.empty((n, K), dtype=ydt).pin_memory()
+    Xe = torch.empty_like(X)
+    e2e_steps = max(1, min(args.steps, 10))
+    for _ in range(2):
+        Xe.copy_(Xpin, non_blocking=True)
+        g.spmm(Xe, Y, schedule=sched, stream=stream)
+        Ypin.copy_(Y, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        Xe.copy_(Xpin, non_blocking=True)
+        g.spmm(Xe, Y, schedule=sched, stream=stream)
+        Ypin.copy_(Y, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
+    barrier()
+
+    peak, peak_kind = measured_peak()
+    achieved = B / (k_ms * 1e-3) / 1e9
+    traffic = read_traffic("fused_spmm_rmat20_k128_fp32.txt") if args.workload == "fp32" else \
+        read_traffic("fused_spmm_rmat21_k256_bf16.txt")
+    launches_per_step = 1 if sched in (S.SCHEDULE_AUTO, S.SCHEDULE_FUSED) else None
+    line = {
+        "metric": METRIC, "value": B * world / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if xdt == torch.float32 else "bf16-storage/f32-accum",
+        "data": "synthetic",
+        "config": {"workload": w["desc"], "nodes": n, "nnz": int(info.nnz), "nnz_local": int(info.nnz_local),
+                   "nnz_remote": int(info.nnz_remote), "K": K, "nparts": w["P"], "local_chunks": int(info.local_chunks),
+                   "remote_chunks": int(info.remote_chunks), "parallelism": "replicas x{}".format(world),
+                   "schedule": args.schedule, "alg_bytes_per_step": B,
+                   "l2": "inputs larger than L2 (X {:.0f} MiB, Y {:.0f} MiB); no flush".format(
+                       n * K * s_x / 2 ** 20, n * K * s_y / 2 ** 20),
+                   "prep_seconds": round(t_prep, 1)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
+                     "kernel_ms": k_ms, "frac_of_8TBs": achieved / 8000.0},
+        "e2e": {"value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": n * K * s_x,
+                "d2h_bytes_per_step": n * K * s_y, "ms_per_step": e2e_ms},
+        "gpu_launches": (launches_per_step * args.steps) if launches_per_step else None,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+        rp, ci, _ = oracle.global_csr(n, row, col, val)
+        nth = host_threads()
+        dt, rows, nnz, kind, rows_per = calibrated_cpu(rp, ci, Xh, K, nth, target_s=2.0)
+        reps = 3
+        tt = []
+        for _ in range(reps):
+            tt.append(cpu_sample(rp, ci, Xh, K, nth, 2.0, rows_per)[0])
+        dt = statistics.median(tt)
+        Bc = alg_bytes(nnz, rows, K, 4, 4)
+        line["cpu_baseline"] = {"value": Bc / dt / 1e9, "unit": "GB/s", "cores": nth, "kind": kind,
+                                "sample": "SAG_reference_host (include/utils.cuh:45-69) over {} threads x {} rows "
+                                          "spread over the matrix ({} nnz), FP32 X, median of {}".format(
+                                              nth, rows_per, nnz, reps)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="fp32", choices=sorted(WORKLOADS))
+    ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "buffer"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, w)
+    return run_ours(args, w)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

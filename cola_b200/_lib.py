@@ -1,0 +1,120 @@
+"""ctypes binding of libcola_b200.so (the C ABI declared in include/cola_spmm.h).
+
+The library is built in-tree (cola_b200/lib/).  Loading fails loudly when it
+is missing: there is no fallback implementation.
+"""
+import ctypes
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libcola_b200.so")
+
+P = ctypes.c_void_p
+I32 = ctypes.c_int32
+I64 = ctypes.c_int64
+F64 = ctypes.c_double
+
+SUCCESS = 0
+STATUS = {0: "success", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "unsupported",
+          5: "I/O error", 6: "over memory budget", 7: "timed out", 8: "not ready", 9: "cancelled"}
+
+FLOAT32 = 0
+BFLOAT16 = 1
+
+SCHEDULE_AUTO = 0
+SCHEDULE_FUSED = 1
+SCHEDULE_BUFFER = 2
+SCHEDULE_PIPELINE = 3
+
+
+class ColaError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("{} ({}): {}".format(STATUS.get(status, "status %d" % status), status, msg))
+        self.status = status
+
+
+class PartitionView(ctypes.Structure):
+    _fields_ = [("part", I32), ("nparts", I32), ("num_nodes", I32), ("nodes_per_part", I32), ("row_lb", I32),
+                ("row_ub", I32),
+                ("csr_rowPtr_l", P), ("csr_colIdx_l", P), ("csr_val_l", P), ("csr_rowIdx_l", P),
+                ("csc_colPtr_r", P), ("csc_rowIdx_r", P), ("csc_val_r", P), ("csc_colIdx_r", P),
+                ("n_rowPtr_l", I64), ("nnz_l", I64), ("n_rows_l", I64), ("n_colPtr_r", I64), ("nnz_r", I64),
+                ("n_cols_r", I64)]
+
+
+class UploadOpts(ctypes.Structure):
+    _fields_ = [("if_split", I32), ("group_size", I32), ("reserved", I32 * 6)]
+
+
+class GraphInfo(ctypes.Structure):
+    _fields_ = [("num_nodes", I32), ("nparts", I32), ("nodes_per_part", I32), ("group_size", I32),
+                ("nnz", I64), ("nnz_local", I64), ("nnz_remote", I64), ("local_chunks", I64),
+                ("remote_chunks", I64), ("remote_cols", I64), ("device_bytes", I64)]
+
+
+class ZipView(ctypes.Structure):
+    _fields_ = [("csr_rowPtr", P), ("csr_colIdx", P), ("csr_rowIdx_zip", P), ("csr_val", P),
+                ("csc_colPtr", P), ("csc_rowIdx", P), ("csc_colIdx_zip", P), ("csc_val", P),
+                ("local_chunks", I32), ("remote_chunks", I32), ("nnz_l", I64), ("nnz_r", I64)]
+
+
+class SpmmOpts(ctypes.Structure):
+    _fields_ = [("accumulate", I32), ("schedule", I32), ("gather_batch_rows", I32), ("reserved", I32 * 5)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "cola_status_string": (ctypes.c_char_p, [I32]),
+    "cola_last_error": (ctypes.c_char_p, []),
+    "cola_version": (ctypes.c_char_p, []),
+    "cola_partition_build": (I32, [I32, I64, P, P, P, I32, P]),
+    "cola_partition_set_free": (None, [P]),
+    "cola_partition_get": (I32, [P, I32, P]),
+    "cola_nnz_split": (I32, [P, I64, P, I64, P, P, I64, P]),
+    "cola_global_csr": (I32, [I32, I64, P, P, P, P, P, P, P]),
+    "cola_workgroup_cols": (I32, [I32, I64, P, P, I32, I32, I32, P, P]),
+    "cola_stage_tables": (I32, [I32, I32, I32, I32, P, I64, I64, P, P, P, P, P, P, P, I64, P, P, I64]),
+    "cola_bin_read_i32": (I32, [ctypes.c_char_p, P, I64, P]),
+    "cola_bin_write_i32": (I32, [ctypes.c_char_p, P, I64]),
+    "cola_bin_read_f32": (I32, [ctypes.c_char_p, P, I64, P]),
+    "cola_bin_write_f32": (I32, [ctypes.c_char_p, P, I64]),
+    "cola_partition_write_bin": (I32, [P, ctypes.c_char_p]),
+    "cola_partition_read_bin": (I32, [ctypes.c_char_p, I32, I32, P]),
+    "cola_rmat_generate": (I32, [I32, F64, F64, F64, F64, ctypes.c_uint64, I32, I32, P, P, P, I64, P]),
+    "cola_ppl0_batch_spmm": (I32, [P, P] + [P] * 8 + [I32] * 7 + [P]),
+    "cola_ppl0_batch_spmm_seq": (I32, [P, P] + [P] * 8 + [I32] * 7 + [P]),
+    "cola_ppl0_batch_buffer_spmm": (I32, [P, P, P] + [P] * 8 + [I32] * 7 + [P]),
+    "cola_ppl_batch_spmm": (I32, [P, P, P, P, P, P] + [I32] * 5 + [P] + [I32] * 5 + [P]),
+    "cola_batching_data_ppl": (I32, [P, P, P, I32, I32, I32, I32, P]),
+    "cola_graph_upload": (I32, [P, P, P, P]),
+    "cola_graph_free": (I32, [P]),
+    "cola_graph_get_info": (I32, [P, P]),
+    "cola_graph_zip_view": (I32, [P, I32, P]),
+    "cola_spmm": (I32, [P, P, I32, I64, P, I32, I64, I32, P, P]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("cola_b200 native library missing at {}: run `python -m cola_b200._build` "
+                               "(or __graft_entry__.build())".format(LIB_PATH))
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status):
+    """Raise ColaError for a non-success status with the library's message."""
+    if status != SUCCESS:
+        msg = lib().cola_last_error()
+        raise ColaError(status, msg.decode() if msg else "")
+    return status

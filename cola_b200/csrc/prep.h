@@ -1,0 +1,42 @@
+// Host-side partition structures and preprocessing steps (see prep.cpp).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "cola_spmm.h"
+
+namespace cola {
+
+// One virtual partition as prep_torch_par.py:24-79 writes it, plus values.
+struct PartHost {
+    int32_t part = 0, row_lb = 0, row_ub = 0;
+    std::vector<int32_t> l_rowPtr, l_colIdx, l_rowIdx;  // local CSR (col % npp), non-empty rows
+    std::vector<float> l_val;
+    std::vector<int32_t> r_colPtr, r_rowIdx, r_colIdx;  // remote CSC (global cols), non-empty cols
+    std::vector<float> r_val;
+};
+
+// Tables of src/distSpMM_ppl_batch.cu:101-193 for one PE.
+struct StageTables {
+    int32_t nstages = 1;
+    std::vector<int32_t> local_offset, remote_offset, put_offset;  // 2*nstages each
+    std::vector<std::vector<int32_t>> idx_ppl;                      // stages 1..nstages-1
+    std::vector<std::vector<int32_t>> put_colIdx;                   // stages 0..nstages-2
+};
+
+cola_status partition_build(int32_t N, int64_t nnz, const int32_t *row, const int32_t *col, const float *val,
+                            int32_t nparts, cola_partition_set *&out);
+cola_status nnz_split(const int32_t *rowIdx, int64_t nrows, const int32_t *rowPtr, int64_t nnz,
+                      std::vector<int32_t> &target, std::vector<int32_t> &ptr);
+cola_status stage_tables(int32_t me, int32_t nranks, int32_t gs, int32_t N, const int32_t *zr, int64_t nrc,
+                         int64_t nchunks_l, const int32_t *wg_cols, const int64_t *wg_off, StageTables &t);
+cola_status workgroup_cols(int32_t N, int64_t nnz, const int32_t *row, const int32_t *col, int32_t nparts,
+                           int32_t gs, int32_t stage, std::vector<int32_t> &out);
+cola_status validate_partition(const cola_partition_set &s, const PartHost &P);
+
+}  // namespace cola
+
+struct cola_partition_set {
+    int32_t num_nodes = 0, nparts = 0, npp = 0;
+    std::vector<cola::PartHost> parts;
+};

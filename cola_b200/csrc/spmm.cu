@@ -1,0 +1,890 @@
+// Launchers, kernel-level C ABI and the device-resident graph of the
+// partitioned SpMM (sm_100a).
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "common.h"
+#include "prep.h"
+#include "spmm_kernels.cuh"
+
+using cola::dev::GatherSeg;
+using cola::dev::PartDesc;
+
+namespace cola {
+
+#define COLA_CUDA(expr)                                                                                   \
+    do {                                                                                                  \
+        cudaError_t _e = (expr);                                                                          \
+        if (_e != cudaSuccess)                                                                            \
+            return ::cola::fail(_e == cudaErrorMemoryAllocation ? COLA_ERROR_OUT_OF_MEMORY : COLA_ERROR_CUDA, \
+                                "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, __LINE__);    \
+    } while (0)
+
+static int sm_count()
+{
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64)
+        dev = 0;
+    if (!cached[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = n > 0 ? n : 148;
+    }
+    return cached[dev];
+}
+
+// Resident blocks per SM for a kernel (cached by function address).
+static int blocks_per_sm(const void *fn, int threads)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void *, int> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(fn);
+    if (it != cache.end())
+        return it->second;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, 0) != cudaSuccess || n <= 0)
+        n = 1;
+    cache[fn] = n;
+    return n;
+}
+
+static int64_t grid_for(const void *fn, int64_t items)
+{
+    const int64_t need = (items + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock;
+    const int64_t full = (int64_t)sm_count() * blocks_per_sm(fn, dev::kThreads);
+    return std::max<int64_t>(1, std::min(need, full));
+}
+
+static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+static int next_pow2(int v)
+{
+    int p = 1;
+    while (p < v)
+        p <<= 1;
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// fused kernel dispatch
+// ---------------------------------------------------------------------------
+struct FusedArgs {
+    const PartDesc *parts;  // device table, or nullptr to use `single`
+    PartDesc single;
+    int nparts;
+    int64_t total;
+    const void *X;
+    int64_t ldx;
+    float *Y;
+    int64_t ldy;
+    int K;
+    cola_dtype xdt;
+    bool vec;  // 16-byte vector path allowed
+};
+
+template <typename TR, int LG, int NV, int UNROLL, bool VEC_Y>
+static cola_status launch_fused_t(const FusedArgs &a, cudaStream_t st)
+{
+    using T = typename dev::ElemOf<TR>::T;
+    constexpr int W = LG * NV * TR::E;
+    auto fn = dev::fused_spmm_kernel<TR, LG, NV, UNROLL, VEC_Y>;
+    const int64_t gx = grid_for((const void *)fn, a.total);
+    const int gy = (a.K + W - 1) / W;
+    fn<<<dim3((unsigned)gx, (unsigned)gy), dev::kThreads, 0, st>>>(a.parts, a.single, a.nparts, a.total,
+                                                                   static_cast<const T *>(a.X), a.ldx, a.Y, a.ldy,
+                                                                   a.K);
+    COLA_CUDA(cudaGetLastError());
+    return COLA_SUCCESS;
+}
+
+template <typename TR, bool VEC_Y>
+static cola_status launch_fused_geo(const FusedArgs &a, int V, cudaStream_t st)
+{
+    // V = vectors (of TR::E elements) per row
+    if (V <= 1)
+        return launch_fused_t<TR, 1, 1, 4, VEC_Y>(a, st);
+    if (V <= 2)
+        return launch_fused_t<TR, 2, 1, 4, VEC_Y>(a, st);
+    if (V <= 4)
+        return launch_fused_t<TR, 4, 1, 4, VEC_Y>(a, st);
+    if (V <= 8)
+        return launch_fused_t<TR, 8, 1, 4, VEC_Y>(a, st);
+    if (V <= 16)
+        return launch_fused_t<TR, 16, 1, 4, VEC_Y>(a, st);
+    if (V <= 32)
+        return launch_fused_t<TR, 32, 1, 4, VEC_Y>(a, st);
+    if (V <= 64)
+        return launch_fused_t<TR, 32, 2, 2, VEC_Y>(a, st);
+    return launch_fused_t<TR, 32, 4, 2, VEC_Y>(a, st);
+}
+
+static cola_status launch_fused(const FusedArgs &a, cudaStream_t st)
+{
+    if (a.total <= 0 || a.K <= 0)
+        return COLA_SUCCESS;
+    if (a.xdt == COLA_FLOAT32) {
+        if (a.vec)
+            return launch_fused_geo<dev::VecTraits<float>, true>(a, a.K / 4, st);
+        return launch_fused_geo<dev::ScalarTraits<float>, false>(a, a.K, st);
+    }
+    if (a.vec)
+        return launch_fused_geo<dev::VecTraits<__nv_bfloat16>, true>(a, a.K / 8, st);
+    return launch_fused_geo<dev::ScalarTraits<__nv_bfloat16>, false>(a, a.K, st);
+}
+
+// Whether the 16-byte vector path applies to X (and staged rows) / Y.
+static bool vec_ok(cola_dtype xdt, const void *X, int64_t ldx, const void *stage, int64_t ld_stage, const float *Y,
+                   int64_t ldy, int K)
+{
+    const int E = xdt == COLA_FLOAT32 ? 4 : 8;
+    if (K % E || ldx % E || !aligned16(X))
+        return false;
+    if (stage && (ld_stage % E || !aligned16(stage)))
+        return false;
+    if (ldy % 4 || !aligned16(Y))
+        return false;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// gather dispatch
+// ---------------------------------------------------------------------------
+static cola_status launch_gather(const GatherSeg *segs, const GatherSeg &single, int nsegs, int64_t total,
+                                 const void *src, int64_t ld_src, void *dst, int64_t ld_dst, int K, cola_dtype dt,
+                                 cudaStream_t st)
+{
+    if (total <= 0 || K <= 0)
+        return COLA_SUCCESS;
+    const int E = dt == COLA_FLOAT32 ? 4 : 8;
+    const bool vec = K % E == 0 && ld_src % E == 0 && ld_dst % E == 0 && aligned16(src) && aligned16(dst);
+#define COLA_GATHER(TR)                                                                                        \
+    do {                                                                                                       \
+        using T = typename dev::ElemOf<TR>::T;                                                                 \
+        auto fn = dev::gather_rows_kernel<TR>;                                                                 \
+        const int64_t gx = grid_for((const void *)fn, total);                                                 \
+        fn<<<(unsigned)gx, dev::kThreads, 0, st>>>(segs, single, nsegs, total, static_cast<const T *>(src),    \
+                                                   ld_src, static_cast<T *>(dst), ld_dst, K);                 \
+    } while (0)
+    if (dt == COLA_FLOAT32) {
+        if (vec)
+            COLA_GATHER(dev::VecTraits<float>);
+        else
+            COLA_GATHER(dev::ScalarTraits<float>);
+    } else {
+        if (vec)
+            COLA_GATHER(dev::VecTraits<__nv_bfloat16>);
+        else
+            COLA_GATHER(dev::ScalarTraits<__nv_bfloat16>);
+    }
+#undef COLA_GATHER
+    COLA_CUDA(cudaGetLastError());
+    return COLA_SUCCESS;
+}
+
+static PartDesc part_desc_zero()
+{
+    PartDesc d;
+    std::memset(&d, 0, sizeof d);
+    return d;
+}
+
+static cola_status check_dim(int32_t dim, int32_t npp)
+{
+    COLA_REQUIRE(dim >= 1, COLA_ERROR_INVALID_ARGUMENT, "dim must be >= 1 (got %d)", dim);
+    COLA_REQUIRE(npp >= 1, COLA_ERROR_INVALID_ARGUMENT, "nodesPerPE must be >= 1 (got %d)", npp);
+    return COLA_SUCCESS;
+}
+
+}  // namespace cola
+
+using namespace cola;
+
+// ===========================================================================
+// Kernel-level C ABI (drop-ins for include/dist_spmm_ppl_batch.cuh launchers)
+// ===========================================================================
+extern "C" {
+
+cola_status cola_ppl0_batch_spmm(float *output, const float *input, const int32_t *csr_rowPtr_l,
+                                 const int32_t *csr_colIdx_l, const int32_t *csr_rowIdx_zip_l,
+                                 const float *csr_val_l, const int32_t *csc_colPtr_r, const int32_t *csc_rowIdx_r,
+                                 const int32_t *csc_colIdx_zip_r, const float *csc_val_r, int32_t local_row_lb,
+                                 int32_t remote_col_lb, int32_t local_row_num, int32_t remote_col_num, int32_t dim,
+                                 int32_t nodesPerPE, int32_t peid, cola_stream_t stream)
+{
+    (void)local_row_lb;  // unused by the reference kernel too (dist_spmm_ppl_batch.cuh:164-167)
+    COLA_TRY(check_dim(dim, nodesPerPE));
+    COLA_REQUIRE(local_row_num >= 0 && remote_col_num >= 0 && remote_col_lb >= 0 && peid >= 0,
+                 COLA_ERROR_INVALID_ARGUMENT, "cola_ppl0_batch_spmm: negative count or offset");
+    const int64_t T = (int64_t)local_row_num + remote_col_num;
+    if (T == 0)
+        return COLA_SUCCESS;  // :232
+    COLA_REQUIRE(output && input, COLA_ERROR_INVALID_ARGUMENT, "cola_ppl0_batch_spmm: null dense pointer");
+    COLA_REQUIRE(local_row_num == 0 || (csr_rowPtr_l && csr_colIdx_l && csr_rowIdx_zip_l && csr_val_l),
+                 COLA_ERROR_INVALID_ARGUMENT, "cola_ppl0_batch_spmm: null local CSR array");
+    COLA_REQUIRE(remote_col_num == 0 || (csc_colPtr_r && csc_rowIdx_r && csc_colIdx_zip_r && csc_val_r),
+                 COLA_ERROR_INVALID_ARGUMENT, "cola_ppl0_batch_spmm: null remote CSC array");
+    PartDesc d = part_desc_zero();
+    d.l_ptr = csr_rowPtr_l;
+    d.l_col = csr_colIdx_l;
+    d.l_row = csr_rowIdx_zip_l;
+    d.l_val = csr_val_l;
+    d.r_ptr = csc_colPtr_r;
+    d.r_row = csc_rowIdx_r;
+    d.r_col = csc_colIdx_zip_r;
+    d.r_val = csc_val_r;
+    d.l_begin = 0;
+    d.l_num = local_row_num;
+    d.r_begin = remote_col_lb;
+    d.r_num = remote_col_num;
+    d.x_local0 = 0;
+    d.x_remote0 = -(int64_t)peid * nodesPerPE;
+    d.r_mode = dev::kRemoteFromX;
+    FusedArgs a{nullptr, d, 1, T, input, dim, output, dim, dim, COLA_FLOAT32,
+                vec_ok(COLA_FLOAT32, input, dim, nullptr, 0, output, dim, dim)};
+    return launch_fused(a, (cudaStream_t)stream);
+}
+
+cola_status cola_ppl0_batch_spmm_seq(float *output, const float *input, const int32_t *csr_rowPtr_l,
+                                     const int32_t *csr_colIdx_l, const int32_t *csr_rowIdx_zip_l,
+                                     const float *csr_val_l, const int32_t *csc_colPtr_r,
+                                     const int32_t *csc_rowIdx_r, const int32_t *csc_colIdx_zip_r,
+                                     const float *csc_val_r, int32_t local_row_lb, int32_t remote_col_lb,
+                                     int32_t local_row_num, int32_t remote_col_num, int32_t dim,
+                                     int32_t nodesPerPE, int32_t peid, cola_stream_t stream)
+{
+    return cola_ppl0_batch_spmm(output, input, csr_rowPtr_l, csr_colIdx_l, csr_rowIdx_zip_l, csr_val_l,
+                                csc_colPtr_r, csc_rowIdx_r, csc_colIdx_zip_r, csc_val_r, local_row_lb,
+                                remote_col_lb, local_row_num, remote_col_num, dim, nodesPerPE, peid, stream);
+}
+
+cola_status cola_ppl0_batch_buffer_spmm(float *output, const float *input, float *comm_buffer,
+                                        const int32_t *csr_rowPtr_l, const int32_t *csr_colIdx_l,
+                                        const int32_t *csr_rowIdx_zip_l, const float *csr_val_l,
+                                        const int32_t *csc_colPtr_r, const int32_t *csc_rowIdx_r,
+                                        const int32_t *csc_colIdx_zip_r, const float *csc_val_r,
+                                        int32_t local_row_lb, int32_t remote_col_lb, int32_t local_row_num,
+                                        int32_t remote_col_num, int32_t dim, int32_t nodesPerPE, int32_t peid,
+                                        cola_stream_t stream)
+{
+    (void)local_row_lb;
+    COLA_TRY(check_dim(dim, nodesPerPE));
+    COLA_REQUIRE(local_row_num >= 0 && remote_col_num >= 0 && remote_col_lb >= 0 && peid >= 0,
+                 COLA_ERROR_INVALID_ARGUMENT, "cola_ppl0_batch_buffer_spmm: negative count or offset");
+    const int64_t T = (int64_t)local_row_num + remote_col_num;
+    if (T == 0)
+        return COLA_SUCCESS;
+    COLA_REQUIRE(output && input && (remote_col_num == 0 || comm_buffer), COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_ppl0_batch_buffer_spmm: null dense pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    float *stage = comm_buffer ? comm_buffer + (int64_t)remote_col_lb * dim : nullptr;
+    if (remote_col_num > 0) {
+        GatherSeg s;
+        std::memset(&s, 0, sizeof s);
+        s.idx = csc_colIdx_zip_r + remote_col_lb;
+        s.n = remote_col_num;
+        s.src_row0 = -(int64_t)peid * nodesPerPE;
+        s.dst_row0 = 0;
+        COLA_TRY(launch_gather(nullptr, s, 1, remote_col_num, input, dim, stage, dim, dim, COLA_FLOAT32, st));
+    }
+    PartDesc d = part_desc_zero();
+    d.l_ptr = csr_rowPtr_l;
+    d.l_col = csr_colIdx_l;
+    d.l_row = csr_rowIdx_zip_l;
+    d.l_val = csr_val_l;
+    d.r_ptr = csc_colPtr_r;
+    d.r_row = csc_rowIdx_r;
+    d.r_col = csc_colIdx_zip_r;
+    d.r_val = csc_val_r;
+    d.l_num = local_row_num;
+    d.r_begin = remote_col_lb;
+    d.r_num = remote_col_num;
+    d.r_mode = dev::kRemoteStagedChunk;
+    d.stage = stage;
+    d.ld_stage = dim;
+    FusedArgs a{nullptr, d, 1, T, input, dim, output, dim, dim, COLA_FLOAT32,
+                vec_ok(COLA_FLOAT32, input, dim, stage, dim, output, dim, dim)};
+    return launch_fused(a, st);
+}
+
+cola_status cola_ppl_batch_spmm(float *output, const float *input, const int32_t *csc_colPtr_r,
+                                const int32_t *csc_rowIdx_r, const int32_t *csc_colIdx_zip_r,
+                                const float *csc_val_r, int32_t local_col_lb, int32_t local_col_ub,
+                                int32_t remote_col_lb, int32_t remote_col_ub, int32_t stage, const int32_t *idx_ppl,
+                                int32_t dim, int32_t nodesPerPE, int32_t group_size, int32_t group_offset,
+                                int32_t peid, cola_stream_t stream)
+{
+    (void)stage;
+    COLA_TRY(check_dim(dim, nodesPerPE));
+    COLA_REQUIRE(group_size >= 1 && remote_col_lb >= 0 && peid >= 0, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_ppl_batch_spmm: bad group_size/offset");
+    const int64_t T = (int64_t)remote_col_ub - remote_col_lb;
+    if (T <= 0)
+        return COLA_SUCCESS;
+    COLA_REQUIRE(output && input && idx_ppl && csc_colPtr_r && csc_rowIdx_r && csc_colIdx_zip_r && csc_val_r,
+                 COLA_ERROR_INVALID_ARGUMENT, "cola_ppl_batch_spmm: null pointer");
+    PartDesc d = part_desc_zero();
+    d.r_ptr = csc_colPtr_r;
+    d.r_row = csc_rowIdx_r;
+    d.r_col = csc_colIdx_zip_r;
+    d.r_val = csc_val_r;
+    d.r_begin = remote_col_lb;
+    d.r_num = (int32_t)T;
+    d.r_mode = dev::kRemoteStageBuffer;
+    d.stage = input;
+    d.ld_stage = dim;
+    d.pe_stride = (int64_t)nodesPerPE * dim;
+    d.idx_ppl = idx_ppl;
+    d.npp = nodesPerPE;
+    d.gs = group_size;
+    d.group_offset = group_offset;
+    d.peid = peid;
+    d.local_col_lb = local_col_lb;
+    d.local_col_ub = local_col_ub;
+    FusedArgs a{nullptr, d, 1, T, input, dim, output, dim, dim, COLA_FLOAT32,
+                vec_ok(COLA_FLOAT32, input, dim, input, dim, output, dim, dim)};
+    return launch_fused(a, (cudaStream_t)stream);
+}
+
+cola_status cola_batching_data_ppl(const float *input, float *send, const int32_t *put_colIdx, int32_t nemb,
+                                   int32_t dim, int32_t nodesPerPE, int32_t group_size, cola_stream_t stream)
+{
+    (void)group_size;
+    COLA_TRY(check_dim(dim, nodesPerPE));
+    if (nemb <= 0)
+        return COLA_SUCCESS;
+    COLA_REQUIRE(input && send && put_colIdx, COLA_ERROR_INVALID_ARGUMENT, "cola_batching_data_ppl: null pointer");
+    GatherSeg s;
+    std::memset(&s, 0, sizeof s);
+    s.idx = put_colIdx;
+    s.n = nemb;
+    s.mod = nodesPerPE;
+    return launch_gather(nullptr, s, 1, nemb, input, dim, send, dim, dim, COLA_FLOAT32, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Device-resident graph
+// ===========================================================================
+struct cola_graph {
+    int device = 0;
+    int32_t N = 0, P = 0, npp = 0, gs = 0, nstages = 1, if_split = 1;
+    int64_t nnz_l = 0, nnz_r = 0, lchunks = 0, rchunks = 0, rcols = 0;
+    void *dmem = nullptr;
+    size_t dbytes = 0;
+    std::vector<cola_zip_view> zips;
+    // fused schedule: all parts, all chunks
+    PartDesc *d_fused = nullptr;
+    int64_t fused_total = 0;
+    std::vector<PartDesc> h_fused;
+    // pipelined schedule (group_size < P)
+    std::vector<cola::StageTables> tables;
+    PartDesc *d_stage0 = nullptr;  // local + intra-group remote of every PE
+    int64_t stage0_total = 0;
+    std::vector<PartDesc *> d_stage;  // stage s >= 1 (index s-1), mode 2
+    std::vector<int64_t> stage_total;
+    std::vector<std::vector<PartDesc>> h_stage;
+    std::vector<GatherSeg *> d_put;  // puts feeding stage s (index s-1)
+    std::vector<int64_t> put_total;
+    std::vector<std::vector<GatherSeg>> h_put;
+    // lazily sized workspaces
+    void *ppl_buf = nullptr;  // 2 x P x npp x K elements
+    size_t ppl_bytes = 0;
+    void *stage_buf = nullptr;  // BUFFER schedule staging
+    size_t stage_bytes = 0;
+    float *ws = nullptr;  // FP32 accumulator for BF16 output
+    size_t ws_bytes = 0;
+    GatherSeg *d_bufsegs = nullptr;  // BUFFER schedule gather segments
+    std::vector<GatherSeg> h_bufsegs;
+};
+
+namespace cola {
+
+static cola_status ensure(void *&p, size_t &have, size_t need)
+{
+    if (have >= need)
+        return COLA_SUCCESS;
+    if (p)
+        COLA_CUDA(cudaFree(p));
+    p = nullptr;
+    have = 0;
+    COLA_CUDA(cudaMalloc(&p, need));
+    have = need;
+    return COLA_SUCCESS;
+}
+
+static void graph_release(cola_graph *g)
+{
+    if (!g)
+        return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(g->device);
+    cudaFree(g->dmem);
+    cudaFree(g->ppl_buf);
+    cudaFree(g->stage_buf);
+    cudaFree(g->ws);
+    cudaSetDevice(cur);
+    delete g;
+}
+
+// Arena: sub-allocations of one device allocation, 256-byte aligned.
+struct Arena {
+    std::vector<std::pair<const void *, size_t>> items;  // host src, bytes
+    std::vector<size_t> offs;
+    size_t total = 0;
+    size_t add(const void *src, size_t bytes)
+    {
+        size_t o = total;
+        items.push_back({src, bytes});
+        offs.push_back(o);
+        total += (bytes + 255) & ~(size_t)255;
+        return o;
+    }
+};
+
+static cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *opts, cola_graph *&out,
+                                cudaStream_t st)
+{
+    COLA_REQUIRE(ps, COLA_ERROR_INVALID_ARGUMENT, "cola_graph_upload: partition set is NULL");
+    const int32_t P = ps->nparts;
+    int32_t gs = opts && opts->group_size > 0 ? opts->group_size : P;
+    const int32_t if_split = opts ? opts->if_split : 1;
+    COLA_REQUIRE(gs >= 1 && gs <= P && P % gs == 0, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_graph_upload: group_size %d must divide nparts %d", gs, P);
+    for (const PartHost &ph : ps->parts)
+        COLA_TRY(validate_partition(*ps, ph));
+    std::unique_ptr<cola_graph, void (*)(cola_graph *)> g(new cola_graph(), graph_release);
+    COLA_CUDA(cudaGetDevice(&g->device));
+    g->N = ps->num_nodes;
+    g->P = P;
+    g->npp = ps->npp;
+    g->gs = gs;
+    g->nstages = P / gs;
+    g->if_split = if_split;
+
+    // split every partition (src/distSpMM_ppl_batch.cu:79-99)
+    struct Split {
+        std::vector<int32_t> l_row, l_ptr, r_col, r_ptr;
+    };
+    std::vector<Split> sp((size_t)P);
+    for (int32_t p = 0; p < P; p++) {
+        const PartHost &ph = ps->parts[(size_t)p];
+        COLA_TRY(nnz_split(ph.l_rowIdx.data(), (int64_t)ph.l_rowIdx.size(), ph.l_rowPtr.data(),
+                           (int64_t)ph.l_colIdx.size(), sp[(size_t)p].l_row, sp[(size_t)p].l_ptr));
+        if (if_split) {
+            COLA_TRY(nnz_split(ph.r_colIdx.data(), (int64_t)ph.r_colIdx.size(), ph.r_colPtr.data(),
+                               (int64_t)ph.r_rowIdx.size(), sp[(size_t)p].r_col, sp[(size_t)p].r_ptr));
+        } else {
+            sp[(size_t)p].r_col = ph.r_colIdx;
+            sp[(size_t)p].r_ptr = ph.r_colIdx.empty() ? std::vector<int32_t>() : ph.r_colPtr;
+        }
+    }
+    // stage tables (pipelined schedule only): work-group column lists are the
+    // sorted unique columns of the group's partitions (= prep_torch_ppl.py:24-49)
+    std::vector<int32_t> wg_cols;
+    std::vector<int64_t> wg_off(1, 0);
+    if (g->nstages > 1) {
+        for (int32_t s = 0; s < g->nstages; s++) {
+            std::vector<int32_t> cols;
+            for (int32_t p = s * gs; p < (s + 1) * gs; p++) {
+                const PartHost &ph = ps->parts[(size_t)p];
+                for (int32_t c : ph.l_colIdx)
+                    cols.push_back((int32_t)((int64_t)p * ps->npp + c));
+                cols.insert(cols.end(), ph.r_colIdx.begin(), ph.r_colIdx.end());
+            }
+            std::sort(cols.begin(), cols.end());
+            cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+            wg_cols.insert(wg_cols.end(), cols.begin(), cols.end());
+            wg_off.push_back((int64_t)wg_cols.size());
+        }
+        g->tables.resize((size_t)P);
+        for (int32_t p = 0; p < P; p++)
+            COLA_TRY(stage_tables(p, P, gs, g->N, sp[(size_t)p].r_col.data(), (int64_t)sp[(size_t)p].r_col.size(),
+                                  (int64_t)sp[(size_t)p].l_row.size(), wg_cols.data(), wg_off.data(),
+                                  g->tables[(size_t)p]));
+    }
+
+    // one device allocation for everything
+    Arena ar;
+    struct Offs {
+        size_t l_ptr, l_col, l_val, l_row, r_ptr, r_row, r_val, r_col;
+    };
+    std::vector<Offs> offs((size_t)P);
+    for (int32_t p = 0; p < P; p++) {
+        const PartHost &ph = ps->parts[(size_t)p];
+        const Split &s = sp[(size_t)p];
+        Offs &o = offs[(size_t)p];
+        o.l_ptr = ar.add(s.l_ptr.data(), s.l_ptr.size() * 4);
+        o.l_col = ar.add(ph.l_colIdx.data(), ph.l_colIdx.size() * 4);
+        o.l_val = ar.add(ph.l_val.data(), ph.l_val.size() * 4);
+        o.l_row = ar.add(s.l_row.data(), s.l_row.size() * 4);
+        o.r_ptr = ar.add(s.r_ptr.data(), s.r_ptr.size() * 4);
+        o.r_row = ar.add(ph.r_rowIdx.data(), ph.r_rowIdx.size() * 4);
+        o.r_val = ar.add(ph.r_val.data(), ph.r_val.size() * 4);
+        o.r_col = ar.add(s.r_col.data(), s.r_col.size() * 4);
+        g->nnz_l += (int64_t)ph.l_colIdx.size();
+        g->nnz_r += (int64_t)ph.r_rowIdx.size();
+        g->lchunks += (int64_t)s.l_row.size();
+        g->rchunks += (int64_t)s.r_col.size();
+        g->rcols += (int64_t)ph.r_colIdx.size();
+    }
+    std::vector<size_t> idx_offs, put_offs;
+    if (g->nstages > 1) {
+        for (int32_t p = 0; p < P; p++) {
+            const StageTables &t = g->tables[(size_t)p];
+            for (const auto &l : t.idx_ppl)
+                idx_offs.push_back(ar.add(l.data(), l.size() * 4));
+            for (const auto &l : t.put_colIdx)
+                put_offs.push_back(ar.add(l.data(), l.size() * 4));
+        }
+    }
+    const size_t desc_fused = ar.add(nullptr, (size_t)P * sizeof(PartDesc));
+    size_t desc_stage0 = 0;
+    std::vector<size_t> desc_stage, desc_put;
+    if (g->nstages > 1) {
+        desc_stage0 = ar.add(nullptr, (size_t)P * sizeof(PartDesc));
+        for (int32_t s = 1; s < g->nstages; s++) {
+            desc_stage.push_back(ar.add(nullptr, (size_t)P * sizeof(PartDesc)));
+            desc_put.push_back(ar.add(nullptr, (size_t)P * sizeof(GatherSeg)));
+        }
+    }
+    const size_t desc_buf = ar.add(nullptr, (size_t)P * sizeof(GatherSeg));
+    ar.total = std::max<size_t>(ar.total, 256);
+    COLA_CUDA(cudaMalloc(&g->dmem, ar.total));
+    g->dbytes = ar.total;
+    char *base = static_cast<char *>(g->dmem);
+    auto at = [&](size_t o) { return reinterpret_cast<const int32_t *>(base + o); };
+
+    // descriptors
+    g->zips.resize((size_t)P);
+    g->h_fused.resize((size_t)P);
+    int64_t item = 0;
+    for (int32_t p = 0; p < P; p++) {
+        const Offs &o = offs[(size_t)p];
+        const Split &s = sp[(size_t)p];
+        cola_zip_view &z = g->zips[(size_t)p];
+        z.csr_rowPtr = at(o.l_ptr);
+        z.csr_colIdx = at(o.l_col);
+        z.csr_val = reinterpret_cast<const float *>(base + o.l_val);
+        z.csr_rowIdx_zip = at(o.l_row);
+        z.csc_colPtr = at(o.r_ptr);
+        z.csc_rowIdx = at(o.r_row);
+        z.csc_val = reinterpret_cast<const float *>(base + o.r_val);
+        z.csc_colIdx_zip = at(o.r_col);
+        z.local_chunks = (int32_t)s.l_row.size();
+        z.remote_chunks = (int32_t)s.r_col.size();
+        z.nnz_l = (int64_t)ps->parts[(size_t)p].l_colIdx.size();
+        z.nnz_r = (int64_t)ps->parts[(size_t)p].r_rowIdx.size();
+        PartDesc d = part_desc_zero();
+        d.l_ptr = z.csr_rowPtr;
+        d.l_col = z.csr_colIdx;
+        d.l_row = z.csr_rowIdx_zip;
+        d.l_val = z.csr_val;
+        d.r_ptr = z.csc_colPtr;
+        d.r_row = z.csc_rowIdx;
+        d.r_col = z.csc_colIdx_zip;
+        d.r_val = z.csc_val;
+        d.l_num = z.local_chunks;
+        d.r_num = z.remote_chunks;
+        d.x_local0 = (int64_t)p * g->npp;
+        d.x_remote0 = 0;
+        d.y_row0 = (int64_t)p * g->npp;
+        d.item0 = item;
+        d.r_mode = dev::kRemoteFromX;
+        item += (int64_t)d.l_num + d.r_num;
+        g->h_fused[(size_t)p] = d;
+    }
+    g->fused_total = item;
+    g->d_fused = reinterpret_cast<PartDesc *>(base + desc_fused);
+    g->h_bufsegs.assign((size_t)P, GatherSeg{});
+    g->d_bufsegs = reinterpret_cast<GatherSeg *>(base + desc_buf);
+
+    std::vector<std::pair<size_t, std::vector<char>>> extra;  // descriptor tables to upload
+    auto push_tbl = [&](size_t off, const void *src, size_t bytes) {
+        extra.push_back({off, std::vector<char>((const char *)src, (const char *)src + bytes)});
+    };
+    push_tbl(desc_fused, g->h_fused.data(), (size_t)P * sizeof(PartDesc));
+
+    if (g->nstages > 1) {
+        // stage 0: local chunks + intra-group remote chunks of every PE
+        std::vector<PartDesc> s0((size_t)P);
+        item = 0;
+        for (int32_t p = 0; p < P; p++) {
+            const StageTables &t = g->tables[(size_t)p];
+            PartDesc d = g->h_fused[(size_t)p];
+            d.l_begin = t.local_offset[0];
+            d.l_num = t.local_offset[1] - t.local_offset[0];
+            d.r_begin = t.remote_offset[0];
+            d.r_num = t.remote_offset[1] - t.remote_offset[0];
+            d.item0 = item;
+            item += (int64_t)d.l_num + d.r_num;
+            s0[(size_t)p] = d;
+        }
+        g->stage0_total = item;
+        g->d_stage0 = reinterpret_cast<PartDesc *>(base + desc_stage0);
+        push_tbl(desc_stage0, s0.data(), s0.size() * sizeof(PartDesc));
+        g->h_stage.assign((size_t)g->nstages - 1, std::vector<PartDesc>((size_t)P));
+        g->h_put.assign((size_t)g->nstages - 1, std::vector<GatherSeg>((size_t)P));
+        for (int32_t s = 1; s < g->nstages; s++) {
+            int64_t it = 0, pit = 0;
+            for (int32_t p = 0; p < P; p++) {
+                const StageTables &t = g->tables[(size_t)p];
+                const size_t io = idx_offs[(size_t)p * (g->nstages - 1) + (s - 1)];
+                PartDesc d = g->h_fused[(size_t)p];
+                d.l_num = 0;
+                d.r_begin = t.remote_offset[2 * s];
+                d.r_num = t.remote_offset[2 * s + 1] - t.remote_offset[2 * s];
+                d.r_mode = dev::kRemoteStageBuffer;
+                d.idx_ppl = at(io);
+                d.npp = g->npp;
+                d.gs = gs;
+                d.group_offset = p / gs * gs;
+                d.peid = p;
+                d.local_col_lb = t.local_offset[2 * s];
+                d.local_col_ub = t.local_offset[2 * s + 1];
+                d.item0 = it;
+                it += d.r_num;
+                g->h_stage[(size_t)s - 1][(size_t)p] = d;
+                // the put that fills stage s's buffer: PE p sends its list
+                // s-1 to target (p - s*gs) mod P  (dist_spmm_ppl_batch.cuh:788-793, 811-816)
+                const size_t po = put_offs[(size_t)p * (g->nstages - 1) + (s - 1)];
+                GatherSeg q;
+                std::memset(&q, 0, sizeof q);
+                q.idx = at(po);
+                q.n = (int64_t)t.put_colIdx[(size_t)s - 1].size();
+                q.src_row0 = 0;  // put lists hold global columns; X is global
+                const int32_t target = ((p - s * gs) % P + P) % P;
+                q.dst_row0 = (int64_t)target * g->npp;
+                q.item0 = pit;
+                pit += q.n;
+                g->h_put[(size_t)s - 1][(size_t)p] = q;
+            }
+            g->stage_total.push_back(it);
+            g->put_total.push_back(pit);
+            g->d_stage.push_back(reinterpret_cast<PartDesc *>(base + desc_stage[(size_t)s - 1]));
+            g->d_put.push_back(reinterpret_cast<GatherSeg *>(base + desc_put[(size_t)s - 1]));
+            push_tbl(desc_stage[(size_t)s - 1], g->h_stage[(size_t)s - 1].data(), (size_t)P * sizeof(PartDesc));
+            push_tbl(desc_put[(size_t)s - 1], g->h_put[(size_t)s - 1].data(), (size_t)P * sizeof(GatherSeg));
+        }
+    }
+
+    // upload: pack into one pinned-free host image and copy once
+    std::vector<char> img(ar.total, 0);
+    for (size_t i = 0; i < ar.items.size(); i++)
+        if (ar.items[i].first && ar.items[i].second)
+            std::memcpy(img.data() + ar.offs[i], ar.items[i].first, ar.items[i].second);
+    for (auto &e : extra)
+        std::memcpy(img.data() + e.first, e.second.data(), e.second.size());
+    COLA_CUDA(cudaMemcpyAsync(g->dmem, img.data(), ar.total, cudaMemcpyHostToDevice, st));
+    COLA_CUDA(cudaStreamSynchronize(st));
+    out = g.release();
+    return COLA_SUCCESS;
+}
+
+}  // namespace cola
+
+extern "C" {
+
+cola_status cola_graph_upload(const cola_partition_set *parts, const cola_upload_opts *opts, cola_graph **out,
+                              cola_stream_t stream)
+{
+    COLA_REQUIRE(out, COLA_ERROR_INVALID_ARGUMENT, "cola_graph_upload: out is NULL");
+    *out = nullptr;
+    try {
+        return graph_upload(parts, opts, *out, (cudaStream_t)stream);
+    } catch (const std::bad_alloc &) {
+        return fail(COLA_ERROR_OUT_OF_MEMORY, "cola_graph_upload: host allocation failed");
+    }
+}
+
+cola_status cola_graph_free(cola_graph *g)
+{
+    graph_release(g);
+    return COLA_SUCCESS;
+}
+
+cola_status cola_graph_get_info(const cola_graph *g, cola_graph_info *o)
+{
+    COLA_REQUIRE(g && o, COLA_ERROR_INVALID_ARGUMENT, "cola_graph_get_info: null argument");
+    o->num_nodes = g->N;
+    o->nparts = g->P;
+    o->nodes_per_part = g->npp;
+    o->group_size = g->gs;
+    o->nnz_local = g->nnz_l;
+    o->nnz_remote = g->nnz_r;
+    o->nnz = g->nnz_l + g->nnz_r;
+    o->local_chunks = g->lchunks;
+    o->remote_chunks = g->rchunks;
+    o->remote_cols = g->rcols;
+    o->device_bytes = (int64_t)(g->dbytes + g->ppl_bytes + g->stage_bytes + g->ws_bytes);
+    return COLA_SUCCESS;
+}
+
+cola_status cola_graph_zip_view(const cola_graph *g, int32_t part, cola_zip_view *o)
+{
+    COLA_REQUIRE(g && o && part >= 0 && part < g->P, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_graph_zip_view: bad argument (part %d)", part);
+    *o = g->zips[(size_t)part];
+    return COLA_SUCCESS;
+}
+
+cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype xdt, int64_t ldx, void *Y, cola_dtype ydt,
+                      int64_t ldy, int32_t K, const cola_spmm_opts *opts, cola_stream_t stream)
+{
+    COLA_REQUIRE(g, COLA_ERROR_INVALID_ARGUMENT, "cola_spmm: graph is NULL");
+    COLA_REQUIRE(K >= 1 && ldx >= K && ldy >= K, COLA_ERROR_INVALID_ARGUMENT, "cola_spmm: K=%d ldx=%lld ldy=%lld",
+                 K, (long long)ldx, (long long)ldy);
+    COLA_REQUIRE((xdt == COLA_FLOAT32 || xdt == COLA_BFLOAT16) && (ydt == COLA_FLOAT32 || ydt == COLA_BFLOAT16),
+                 COLA_ERROR_INVALID_ARGUMENT, "cola_spmm: unknown dtype");
+    COLA_REQUIRE(g->N == 0 || (X && Y), COLA_ERROR_INVALID_ARGUMENT, "cola_spmm: null X or Y");
+    const int accumulate = opts ? opts->accumulate : 0;
+    int schedule = opts ? opts->schedule : COLA_SCHEDULE_AUTO;
+    const int batch_rows = opts && opts->gather_batch_rows > 0 ? opts->gather_batch_rows : 4096;
+    COLA_REQUIRE(!(accumulate && ydt != COLA_FLOAT32), COLA_ERROR_UNSUPPORTED,
+                 "cola_spmm: accumulate needs an FP32 Y");
+    if (schedule == COLA_SCHEDULE_AUTO)
+        schedule = g->nstages > 1 ? COLA_SCHEDULE_PIPELINE : COLA_SCHEDULE_FUSED;
+    COLA_REQUIRE(schedule != COLA_SCHEDULE_PIPELINE || g->nstages > 1, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_spmm: the pipelined schedule needs a graph uploaded with group_size < nparts");
+    int cur = 0;
+    COLA_CUDA(cudaGetDevice(&cur));
+    COLA_REQUIRE(cur == g->device, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_spmm: graph lives on device %d, current device is %d", g->device, cur);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->N == 0)
+        return COLA_SUCCESS;
+
+    // accumulation target
+    float *acc = nullptr;
+    int64_t ldacc = 0;
+    if (ydt == COLA_FLOAT32) {
+        acc = static_cast<float *>(Y);
+        ldacc = ldy;
+    } else {
+        COLA_TRY(ensure(reinterpret_cast<void *&>(g->ws), g->ws_bytes, (size_t)g->N * K * sizeof(float)));
+        acc = g->ws;
+        ldacc = K;
+    }
+    if (!accumulate) {
+        if (ldacc == K)
+            COLA_CUDA(cudaMemsetAsync(acc, 0, (size_t)g->N * K * sizeof(float), st));
+        else
+            COLA_CUDA(cudaMemset2DAsync(acc, (size_t)ldacc * sizeof(float), 0, (size_t)K * sizeof(float),
+                                        (size_t)g->N, st));
+    }
+    const size_t esz = xdt == COLA_FLOAT32 ? 4 : 2;
+    const int P = g->P;
+
+    if (schedule == COLA_SCHEDULE_FUSED) {
+        FusedArgs a{g->d_fused, part_desc_zero(), P, g->fused_total, X, ldx, acc, ldacc, K, xdt,
+                    vec_ok(xdt, X, ldx, nullptr, 0, acc, ldacc, K)};
+        COLA_TRY(launch_fused(a, st));
+    } else if (schedule == COLA_SCHEDULE_BUFFER) {
+        // local chunks of every partition, then per partition the remote rows in
+        // batches: gather into the HBM staging buffer, scatter from it.
+        const int64_t ldst = (K + 7) / 8 * 8;
+        COLA_TRY(ensure(g->stage_buf, g->stage_bytes, (size_t)2 * batch_rows * ldst * esz));
+        // one launch for the local parts: r_num = 0 via a host copy of the table
+        {
+            FusedArgs a{nullptr, part_desc_zero(), 1, 0, X, ldx, acc, ldacc, K, xdt,
+                        vec_ok(xdt, X, ldx, nullptr, 0, acc, ldacc, K)};
+            for (int32_t p = 0; p < P; p++) {
+                PartDesc d = g->h_fused[(size_t)p];
+                d.r_num = 0;
+                d.item0 = 0;
+                a.single = d;
+                a.total = d.l_num;
+                COLA_TRY(launch_fused(a, st));
+            }
+        }
+        int pp = 0;
+        for (int32_t p = 0; p < P; p++) {
+            const PartDesc &full = g->h_fused[(size_t)p];
+            for (int32_t b0 = 0; b0 < full.r_num; b0 += batch_rows) {
+                const int32_t nb = std::min(batch_rows, full.r_num - b0);
+                char *sb = static_cast<char *>(g->stage_buf) + (size_t)(pp & 1) * batch_rows * ldst * esz;
+                pp++;
+                GatherSeg s;
+                std::memset(&s, 0, sizeof s);
+                s.idx = full.r_col + b0;
+                s.n = nb;
+                COLA_TRY(launch_gather(nullptr, s, 1, nb, X, ldx, sb, ldst, K, xdt, st));
+                PartDesc d = full;
+                d.l_num = 0;
+                d.r_begin = b0;
+                d.r_num = nb;
+                d.item0 = 0;
+                d.r_mode = dev::kRemoteStagedChunk;
+                d.stage = sb;
+                d.ld_stage = ldst;
+                FusedArgs a{nullptr, d, 1, nb, X, ldx, acc, ldacc, K, xdt,
+                            vec_ok(xdt, X, ldx, sb, ldst, acc, ldacc, K)};
+                COLA_TRY(launch_fused(a, st));
+            }
+        }
+    } else {  // PIPELINE
+        const int64_t ld = ldx;
+        const size_t per_pe = (size_t)g->npp * ld * esz;
+        COLA_TRY(ensure(g->ppl_buf, g->ppl_bytes, 2 * (size_t)P * per_pe));
+        // stage 0: local + intra-group remote of every PE (.cuh:797-805)
+        {
+            FusedArgs a{g->d_stage0, part_desc_zero(), P, g->stage0_total, X, ldx, acc, ldacc, K, xdt,
+                        vec_ok(xdt, X, ldx, nullptr, 0, acc, ldacc, K)};
+            COLA_TRY(launch_fused(a, st));
+        }
+        for (int32_t s = 1; s < g->nstages; s++) {
+            char *buf = static_cast<char *>(g->ppl_buf) + (size_t)((s - 1) % 2) * P * per_pe;
+            // every PE's put for stage s (batching_data_ppl + put_nbi, .cuh:788-793/811-816)
+            COLA_TRY(launch_gather(g->d_put[(size_t)s - 1], GatherSeg{}, P, g->put_total[(size_t)s - 1], X, ldx,
+                                   buf, ld, K, xdt, st));
+            // stage s compute of every PE (.cuh:822-835)
+            // each PE reads its own copy of the buffer (PE p's copy at p * npp rows)
+            std::vector<PartDesc> &hs = g->h_stage[(size_t)s - 1];
+            bool stage_ok = true;
+            for (int32_t p = 0; p < P; p++) {
+                const PartDesc &d = hs[(size_t)p];
+                if (d.stage != buf + (size_t)p * per_pe || d.ld_stage != ld || d.pe_stride != (int64_t)g->npp * ld) {
+                    stage_ok = false;
+                    break;
+                }
+            }
+            if (!stage_ok) {
+                for (int32_t p = 0; p < P; p++) {
+                    PartDesc &d = hs[(size_t)p];
+                    d.stage = buf + (size_t)p * per_pe;
+                    d.ld_stage = ld;
+                    d.pe_stride = (int64_t)g->npp * ld;
+                }
+                COLA_CUDA(cudaMemcpyAsync(g->d_stage[(size_t)s - 1], hs.data(), hs.size() * sizeof(PartDesc),
+                                          cudaMemcpyHostToDevice, st));
+                COLA_CUDA(cudaStreamSynchronize(st));
+            }
+            FusedArgs a{g->d_stage[(size_t)s - 1], part_desc_zero(), P, g->stage_total[(size_t)s - 1], X, ldx, acc,
+                        ldacc, K, xdt, vec_ok(xdt, X, ldx, buf, ld, acc, ldacc, K)};
+            COLA_TRY(launch_fused(a, st));
+        }
+    }
+
+    if (ydt == COLA_BFLOAT16) {
+        const int64_t n = (int64_t)g->N * K;
+        const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 8);
+        dev::f32_to_bf16_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), dev::kThreads, 0, st>>>(
+            acc, ldacc, static_cast<__nv_bfloat16 *>(Y), ldy, g->N, K);
+        COLA_CUDA(cudaGetLastError());
+    }
+    return COLA_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,349 @@
+// Device code of the partitioned SpMM (sm_100a).
+//
+// One warp owns one work item: a local CSR chunk (gather-FMA over its
+// entries, include/dist_spmm_ppl_batch.cuh:164-197) or a remote CSC chunk
+// (one staged dense row scattered to every row of the chunk, :112-160).
+// Feature rows move as 16-byte vectors: a lane owns NV vectors of E elements
+// (E = 4 FP32 or 8 BF16), LG lanes cover one row tile and G = 32/LG groups of a
+// warp work on different entries of the same chunk at once (narrow K), their
+// partial sums combined with warp shuffles before the single write.
+// Accumulation is FP32 in registers; writes into Y are 16-byte vector
+// reductions (red.global.add.v4.f32 via atomicAdd(float4*)).
+#pragma once
+#include <cstdint>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace cola {
+namespace dev {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarpsPerBlock = 8;
+constexpr int kThreads = kWarpsPerBlock * 32;
+
+// Where a remote chunk's dense row comes from.
+enum RemoteMode : int32_t {
+    kRemoteFromX = 0,       // X[x_remote0 + global col]           (on-chip staging)
+    kRemoteStagedChunk = 1, // stage[c - r_begin]                  (HBM staging buffer)
+    kRemoteStageBuffer = 2  // pipeline buffer row idx_ppl[w] of this PE or a group peer
+};
+
+// One virtual partition's slice of a launch.
+struct PartDesc {
+    const int32_t *l_ptr, *l_col, *l_row;
+    const float *l_val;
+    const int32_t *r_ptr, *r_row, *r_col;
+    const float *r_val;
+    int32_t l_begin, l_num, r_begin, r_num;
+    int64_t x_local0;   // X row holding local column 0
+    int64_t x_remote0;  // X row holding global column 0
+    int64_t y_row0;     // Y row holding partition row 0
+    int64_t item0;      // first launch item of this partition (prefix over parts)
+    int32_t r_mode;
+    int32_t npp, gs, group_offset, peid, local_col_lb, local_col_ub, pad_;
+    const void *stage;  // staged rows (modes 1, 2)
+    int64_t ld_stage;   // elements between staged rows
+    int64_t pe_stride;  // elements between PEs' copies of the stage buffer (mode 2)
+    const int32_t *idx_ppl;
+};
+
+template <typename T>
+struct VecTraits;
+
+template <>
+struct VecTraits<float> {
+    static constexpr int E = 4;
+    using raw_t = float4;
+    __device__ __forceinline__ static raw_t load(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+    __device__ __forceinline__ static raw_t zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+    __device__ __forceinline__ static void unpack(const raw_t &r, float (&f)[E])
+    {
+        f[0] = r.x;
+        f[1] = r.y;
+        f[2] = r.z;
+        f[3] = r.w;
+    }
+};
+
+template <>
+struct VecTraits<__nv_bfloat16> {
+    static constexpr int E = 8;
+    using raw_t = uint4;
+    __device__ __forceinline__ static raw_t load(const __nv_bfloat16 *p)
+    {
+        return __ldg(reinterpret_cast<const uint4 *>(p));
+    }
+    __device__ __forceinline__ static raw_t zero() { return make_uint4(0u, 0u, 0u, 0u); }
+    // BF16 -> FP32 is exact: the 16 bits become the high half of the float.
+    __device__ __forceinline__ static void unpack(const raw_t &r, float (&f)[E])
+    {
+        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            f[2 * i] = __uint_as_float(w[i] << 16);
+            f[2 * i + 1] = __uint_as_float(w[i] & 0xffff0000u);
+        }
+    }
+};
+
+// Scalar fallback (rows not 16-byte aligned or K not a multiple of E).
+template <typename T>
+struct ScalarTraits {
+    static constexpr int E = 1;
+    using raw_t = T;
+    __device__ __forceinline__ static raw_t load(const T *p) { return *p; }
+    __device__ __forceinline__ static raw_t zero() { return T(0.f); }
+    __device__ __forceinline__ static void unpack(const raw_t &r, float (&f)[1]) { f[0] = (float)r; }
+};
+
+template <typename TR>
+struct ElemOf;
+template <>
+struct ElemOf<VecTraits<float>> {
+    using T = float;
+};
+template <>
+struct ElemOf<VecTraits<__nv_bfloat16>> {
+    using T = __nv_bfloat16;
+};
+template <typename U>
+struct ElemOf<ScalarTraits<U>> {
+    using T = U;
+};
+
+// Y[p..p+E) += a[0..E): 16-byte vector reductions when E is a multiple of 4.
+template <int E, bool VEC_Y>
+__device__ __forceinline__ void red_add(float *p, const float (&a)[E])
+{
+    if constexpr (VEC_Y && (E % 4) == 0) {
+#pragma unroll
+        for (int q = 0; q < E / 4; q++)
+            atomicAdd(reinterpret_cast<float4 *>(p + 4 * q), make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]));
+    } else {
+#pragma unroll
+        for (int q = 0; q < E; q++)
+            atomicAdd(p + q, a[q]);
+    }
+}
+
+// Locate the partition of launch item `it`, moving forward from *p.
+__device__ __forceinline__ const PartDesc *find_part(const PartDesc *parts, int nparts, int64_t it, int &p)
+{
+    while (p + 1 < nparts && it >= parts[p + 1].item0)
+        p++;
+    return parts + p;
+}
+
+// The fused partitioned SpMM: items [0, total) over all parts; item i of part
+// d is local chunk d.l_begin + i when i < d.l_num, else remote chunk
+// d.r_begin + (i - d.l_num).  blockIdx.y selects the feature tile.
+template <typename TR, int LG, int NV, int UNROLL, bool VEC_Y>
+__global__ void __launch_bounds__(kThreads) fused_spmm_kernel(const PartDesc *__restrict__ parts,
+                                                              const __grid_constant__ PartDesc single, int nparts,
+                                                              int64_t total,
+                                                              const typename ElemOf<TR>::T *__restrict__ X,
+                                                              int64_t ldx, float *__restrict__ Y, int64_t ldy, int K)
+{
+    using T = typename ElemOf<TR>::T;
+    using raw_t = typename TR::raw_t;
+    constexpr int E = TR::E;
+    constexpr int G = 32 / LG;
+    constexpr int W = LG * NV * E;  // features per tile
+    const int lane = threadIdx.x & 31;
+    const int g = lane / LG;
+    const int gl = lane % LG;
+    const int k0 = blockIdx.y * W;
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    const int64_t w0 = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    int pidx = 0;
+
+    // features owned by this lane: k0 + (gl + j*LG)*E + e, j < NV
+    bool kok[NV];
+#pragma unroll
+    for (int j = 0; j < NV; j++)
+        kok[j] = (k0 + (gl + j * LG) * E) < K;
+
+    for (int64_t it = w0; it < total; it += nwarps) {
+        const PartDesc &d = parts ? *find_part(parts, nparts, it, pidx) : single;
+        const int64_t li = it - d.item0;
+        if (li < d.l_num) {
+            // ---------------- local CSR chunk ----------------
+            const int64_t c = d.l_begin + li;
+            const int lb = __ldg(d.l_ptr + c), hb = __ldg(d.l_ptr + c + 1);
+            const int row = __ldg(d.l_row + c);
+            float acc[NV][E];
+#pragma unroll
+            for (int j = 0; j < NV; j++)
+#pragma unroll
+                for (int e = 0; e < E; e++)
+                    acc[j][e] = 0.f;
+            const T *xl = X + d.x_local0 * ldx + k0;
+            for (int base = lb; base < hb; base += 32) {
+                const int n = min(32, hb - base);
+                int mc = 0;
+                float mv = 0.f;
+                if (lane < n) {
+                    mc = __ldg(d.l_col + base + lane);
+                    mv = __ldg(d.l_val + base + lane);
+                }
+                for (int jj = 0; jj < n; jj += G * UNROLL) {
+                    raw_t xr[UNROLL][NV];
+                    float vv[UNROLL];
+#pragma unroll
+                    for (int u = 0; u < UNROLL; u++) {
+                        const int k = jj + u * G + g;
+                        const int cc = __shfl_sync(kFull, mc, k & 31);
+                        const float v = __shfl_sync(kFull, mv, k & 31);
+                        const bool ok = k < n;
+                        vv[u] = ok ? v : 0.f;
+                        const T *xp = xl + (int64_t)cc * ldx;
+#pragma unroll
+                        for (int j = 0; j < NV; j++)
+                            xr[u][j] = (ok && kok[j]) ? TR::load(xp + (gl + j * LG) * E) : TR::zero();
+                    }
+#pragma unroll
+                    for (int u = 0; u < UNROLL; u++)
+#pragma unroll
+                        for (int j = 0; j < NV; j++) {
+                            float f[E];
+                            TR::unpack(xr[u][j], f);
+#pragma unroll
+                            for (int e = 0; e < E; e++)
+                                acc[j][e] = fmaf(vv[u], f[e], acc[j][e]);
+                        }
+                }
+            }
+#pragma unroll
+            for (int off = LG; off < 32; off <<= 1)
+#pragma unroll
+                for (int j = 0; j < NV; j++)
+#pragma unroll
+                    for (int e = 0; e < E; e++)
+                        acc[j][e] += __shfl_xor_sync(kFull, acc[j][e], off);
+            if (g == 0) {
+                float *yp = Y + (d.y_row0 + row) * ldy + k0;
+#pragma unroll
+                for (int j = 0; j < NV; j++)
+                    if (kok[j])
+                        red_add<E, VEC_Y>(yp + (gl + j * LG) * E, acc[j]);
+            }
+        } else {
+            // ---------------- remote CSC chunk ----------------
+            const int64_t w = li - d.l_num;
+            const int64_t c = d.r_begin + w;
+            const int lb = __ldg(d.r_ptr + c), hb = __ldg(d.r_ptr + c + 1);
+            const T *src;
+            if (d.r_mode == kRemoteFromX) {
+                src = X + (d.x_remote0 + __ldg(d.r_col + c)) * ldx;
+            } else if (d.r_mode == kRemoteStagedChunk) {
+                src = static_cast<const T *>(d.stage) + w * d.ld_stage;
+            } else {
+                const int32_t col = __ldg(d.r_col + c);
+                const int64_t ix = __ldg(d.idx_ppl + w);
+                int64_t peer_off = 0;
+                if (!(c >= d.local_col_lb && c < d.local_col_ub)) {
+                    const int peer = (col / d.npp) % d.gs + d.group_offset;
+                    peer_off = (int64_t)(peer - d.peid) * d.pe_stride;
+                }
+                src = static_cast<const T *>(d.stage) + peer_off + ix * d.ld_stage;
+            }
+            src += k0;
+            // stage the dense row on chip (registers)
+            float xs[NV][E];
+#pragma unroll
+            for (int j = 0; j < NV; j++) {
+                raw_t r = kok[j] ? TR::load(src + (gl + j * LG) * E) : TR::zero();
+                TR::unpack(r, xs[j]);
+            }
+            for (int base = lb; base < hb; base += 32) {
+                const int n = min(32, hb - base);
+                int mr = 0;
+                float mv = 0.f;
+                if (lane < n) {
+                    mr = __ldg(d.r_row + base + lane);
+                    mv = __ldg(d.r_val + base + lane);
+                }
+                for (int jj = 0; jj < n; jj += G) {
+                    const int k = jj + g;
+                    const int r = __shfl_sync(kFull, mr, k & 31);
+                    const float v = __shfl_sync(kFull, mv, k & 31);
+                    if (k < n) {
+                        float *yp = Y + (d.y_row0 + r) * ldy + k0;
+#pragma unroll
+                        for (int j = 0; j < NV; j++)
+                            if (kok[j]) {
+                                float a[E];
+#pragma unroll
+                                for (int e = 0; e < E; e++)
+                                    a[e] = v * xs[j][e];
+                                red_add<E, VEC_Y>(yp + (gl + j * LG) * E, a);
+                            }
+                    }
+                }
+            }
+        }
+    }
+}
+
+// A segment of a row gather: dst[dst_row0 + b] = src[src_row0 + idx[b] (% mod)].
+struct GatherSeg {
+    const int32_t *idx;
+    int64_t n;
+    int64_t src_row0;
+    int64_t dst_row0;
+    int64_t item0;
+    int32_t mod;  // 0: no modulo
+    int32_t pad_;
+};
+
+// Staged row gather (include/dist_spmm_ppl_batch.cuh:59-73 generalised): one
+// warp per row, 16-byte vectors, rows of all segments in one launch.
+template <typename TR>
+__global__ void __launch_bounds__(kThreads) gather_rows_kernel(const GatherSeg *__restrict__ segs,
+                                                               const __grid_constant__ GatherSeg single, int nsegs,
+                                                               int64_t total,
+                                                               const typename ElemOf<TR>::T *__restrict__ src,
+                                                               int64_t ld_src, typename ElemOf<TR>::T *__restrict__ dst,
+                                                               int64_t ld_dst, int K)
+{
+    using T = typename ElemOf<TR>::T;
+    using raw_t = typename TR::raw_t;
+    constexpr int E = TR::E;
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    int sidx = 0;
+    for (int64_t it = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); it < total; it += nwarps) {
+        const GatherSeg *s = &single;
+        if (segs) {
+            while (sidx + 1 < nsegs && it >= segs[sidx + 1].item0)
+                sidx++;
+            s = segs + sidx;
+        }
+        const int64_t b = it - s->item0;
+        int32_t r = __ldg(s->idx + b);
+        if (s->mod)
+            r %= s->mod;
+        const T *sp = src + (s->src_row0 + r) * ld_src;
+        T *dp = dst + (s->dst_row0 + b) * ld_dst;
+        for (int k = lane * E; k < K; k += 32 * E) {
+            raw_t v = TR::load(sp + k);
+            *reinterpret_cast<raw_t *>(dp + k) = v;
+        }
+    }
+}
+
+// FP32 -> BF16 (round to nearest even) of an n x K block, row strides ld_in/ld_out.
+__global__ void __launch_bounds__(kThreads) f32_to_bf16_kernel(const float *__restrict__ in, int64_t ld_in,
+                                                              __nv_bfloat16 *__restrict__ out, int64_t ld_out,
+                                                              int64_t rows, int K)
+{
+    const int64_t total = rows * (int64_t)K;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / K, k = i % K;
+        out[r * ld_out + k] = __float2bfloat16_rn(in[r * ld_in + k]);
+    }
+}
+
+}  // namespace dev
+}  // namespace cola

@@ -1,0 +1,280 @@
+/*
+ * cola_spmm.h -- C ABI of cola_b200, a single-GPU B200 (sm_100a) implementation
+ * of CoLa's partitioned SpMM (zzzlxhhh/CoLa).
+ *
+ * The matrix is split into P virtual row partitions ("PEs").  Partition p owns
+ * rows [p*npp, min((p+1)*npp, N)), npp = ceil(N/P), and holds
+ *   - a local CSR block over the columns it owns (column ids are col % npp),
+ *   - a remote CSC block over the other columns (global ids), compacted so that
+ *     only non-empty columns appear,
+ * both optionally chunked by nnz_split.  Dense matrices are row-major.
+ *
+ * Symmetric-buffer convention (replaces the NVSHMEM symmetric heap on one GPU):
+ * the P copies of a per-PE dense buffer (the input X slices, the pipeline
+ * buffers) are laid out back to back, nodesPerPE*dim elements apart, so PE q's
+ * copy of a buffer that PE me addresses as `a` is a + (q - me)*nodesPerPE*dim.
+ * For X this means: the whole X is one (P*npp) x dim array and PE me's `input`
+ * points at row me*npp of it.
+ *
+ * Errors: every entry point returns a cola_status and never exits the process
+ * (the reference exits on error: include/utils.cuh:10-22).
+ * cola_last_error() returns a thread-local message for the last failure.
+ * Launch entry points are asynchronous on the given stream, like the
+ * reference's launchers.
+ */
+#ifndef COLA_SPMM_H
+#define COLA_SPMM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Binary-compatible with cudaStream_t. */
+typedef struct CUstream_st *cola_stream_t;
+
+typedef enum cola_status {
+    COLA_SUCCESS = 0,
+    COLA_ERROR_INVALID_ARGUMENT = 1,
+    COLA_ERROR_CUDA = 2,
+    COLA_ERROR_OUT_OF_MEMORY = 3,
+    COLA_ERROR_UNSUPPORTED = 4,
+    COLA_ERROR_IO = 5,
+    COLA_ERROR_BUDGET = 6,
+    COLA_ERROR_TIMEOUT = 7,
+    COLA_ERROR_NOT_READY = 8,
+    COLA_ERROR_CANCELLED = 9
+} cola_status;
+
+typedef enum cola_dtype {
+    COLA_FLOAT32 = 0,
+    COLA_BFLOAT16 = 1
+} cola_dtype;
+
+const char *cola_status_string(cola_status s);
+/* Thread-local description of the last failure in this thread ("" if none). */
+const char *cola_last_error(void);
+/* Library version string. */
+const char *cola_version(void);
+
+/* ========================================================================
+ * Preprocessing (host).  Replaces prep_torch_par.py, prep_torch_ppl.py,
+ * nnz_split and the stage tables of src/distSpMM_ppl_batch.cu; outputs are
+ * bit-identical to the reference's.
+ * ====================================================================== */
+
+typedef struct cola_partition_set cola_partition_set;
+
+/* prep_torch_par.py:24-79 (row_partition) for all nparts partitions, from a
+ * COO list (duplicates allowed; merged as scipy's tocsr()/tocsc() merge them,
+ * their values summed in input order).  val may be NULL (all ones, which is
+ * what the reference uses: src/distSpMM_ppl_batch.cu:83,99). */
+cola_status cola_partition_build(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
+                                 const float *val, int32_t nparts, cola_partition_set **out);
+void cola_partition_set_free(cola_partition_set *s);
+
+/* Read-only view of one partition.  Array lengths follow the reference's .bin
+ * files: n_rowPtr_l = n_rows_l + 1 (1 if no local entries), n_colPtr_r =
+ * n_cols_r + 1 (1 if no remote entries). */
+typedef struct cola_partition_view {
+    int32_t part, nparts, num_nodes, nodes_per_part, row_lb, row_ub;
+    const int32_t *csr_rowPtr_l;  /* n_rowPtr_l */
+    const int32_t *csr_colIdx_l;  /* nnz_l, local column ids (col % npp) */
+    const float *csr_val_l;       /* nnz_l */
+    const int32_t *csr_rowIdx_l;  /* n_rows_l, partition-local row ids */
+    const int32_t *csc_colPtr_r;  /* n_colPtr_r */
+    const int32_t *csc_rowIdx_r;  /* nnz_r, partition-local row ids */
+    const float *csc_val_r;       /* nnz_r */
+    const int32_t *csc_colIdx_r;  /* n_cols_r, global column ids */
+    int64_t n_rowPtr_l, nnz_l, n_rows_l, n_colPtr_r, nnz_r, n_cols_r;
+} cola_partition_view;
+
+cola_status cola_partition_get(const cola_partition_set *s, int32_t part, cola_partition_view *out);
+
+/* include/dist_spmm_ppl_batch.cuh:29-56 (nnz_split).  Chunk granularity is the
+ * average entries per listed row rounded up to a multiple of 32.  Pass
+ * target == NULL to only count (*nchunks).  ptr receives nchunks+1 entries, or
+ * none when nrows == 0 (as the reference leaves it empty). */
+cola_status cola_nnz_split(const int32_t *rowIdx, int64_t nrows, const int32_t *rowPtr, int64_t nnz,
+                           int32_t *target, int32_t *ptr, int64_t capacity, int64_t *nchunks);
+
+/* prep_torch_par.py:93-101 (serialize: global CSR).  rowPtr: num_nodes+1;
+ * colIdx/val: capacity nnz (val may be NULL). */
+cola_status cola_global_csr(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
+                            const float *val_in, int32_t *rowPtr, int32_t *colIdx, float *val_out,
+                            int64_t *nnz_out);
+
+/* prep_torch_ppl.py:24-49: sorted unique columns referenced by work group
+ * `stage` (rows [stage*gs*npp, min((stage+1)*gs*npp, N))).  out capacity:
+ * num_nodes. */
+cola_status cola_workgroup_cols(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
+                                int32_t nparts, int32_t group_size, int32_t stage, int32_t *out,
+                                int64_t *count);
+
+/* src/distSpMM_ppl_batch.cu:101-193: stage offset and index tables of PE `me`.
+ * wg_cols/wg_off: all work groups' column lists concatenated (wg_off has
+ * nranks/group_size + 1 entries; may be NULL when group_size == nranks).
+ * Outputs: local/remote/put offsets (2*nstages each), idx_ppl lists of stages
+ * 1..nstages-1 concatenated with idx_off (nstages entries, idx_off[0] = 0,
+ * stage i list = [idx_off[i-1], idx_off[i])), put lists of stages
+ * 0..nstages-2 concatenated with put_lst_off (nstages entries). */
+cola_status cola_stage_tables(int32_t me, int32_t nranks, int32_t group_size, int32_t num_nodes,
+                              const int32_t *csc_colIdx_zip_r, int64_t n_remote_chunks, int64_t n_local_chunks,
+                              const int32_t *wg_cols, const int64_t *wg_off, int32_t *local_offset_ppl,
+                              int32_t *remote_offset_ppl, int32_t *put_offset_ppl, int32_t *idx_ppl,
+                              int64_t *idx_off, int64_t idx_capacity, int32_t *put_colIdx_ppl,
+                              int64_t *put_lst_off, int64_t put_capacity);
+
+/* include/dist_spmm_ppl_batch.cuh:7-27 (bin2vec) without its 2 GiB int
+ * overflow: raw little-endian int32 files, no header.  Pass out == NULL to
+ * size (*count = file bytes / 4). */
+cola_status cola_bin_read_i32(const char *path, int32_t *out, int64_t capacity, int64_t *count);
+cola_status cola_bin_write_i32(const char *path, const int32_t *data, int64_t n);
+cola_status cola_bin_read_f32(const char *path, float *out, int64_t capacity, int64_t *count);
+cola_status cola_bin_write_f32(const char *path, const float *data, int64_t n);
+
+/* Write the reference's on-disk layout for this partition set
+ * (prep_torch_par.py:56-58,77-79): <dir>/GPU<P>/{csr_rowPtr_l,csr_colIdx_l,
+ * csr_rowIdx_l,csc_colPtr_r,csc_rowIdx_r,csc_colIdx_r}_<P>_<r>.bin, plus
+ * csr_val_l_/csc_val_r_ FP32 files (the reference writes no values). */
+cola_status cola_partition_write_bin(const cola_partition_set *s, const char *dir);
+/* Load a partition set from that layout.  Value files are optional (missing
+ * values load as 1.0, the reference's choice). */
+cola_status cola_partition_read_bin(const char *dir, int32_t num_nodes, int32_t nparts, cola_partition_set **out);
+
+/* Seeded R-MAT graph (a, b, c, 1-a-b-c), scale s -> 2^s nodes.  Draws
+ * undirected non-self-loop edges until avg_degree*N/2 distinct ones exist,
+ * then symmetrises (each edge both ways), optionally adds self-loops, and
+ * sorts by (row, col).  Values: 0 none(1.0), 1 = 1/deg(row), 2 =
+ * 1/sqrt(deg(row)*deg(col)).  Two-call protocol: row == NULL returns *nnz. */
+cola_status cola_rmat_generate(int32_t scale, double avg_degree, double a, double b, double c, uint64_t seed,
+                               int32_t self_loops, int32_t value_kind, int32_t *row, int32_t *col, float *val,
+                               int64_t capacity, int64_t *nnz);
+
+/* ========================================================================
+ * Kernel-level launchers: drop-ins for the reference's launchers in
+ * include/dist_spmm_ppl_batch.cuh, same argument meaning.  FP32, any dim >= 1.
+ * `output` is accumulated into (the caller zeroes it, as the reference's
+ * caller does: src/distSpMM_ppl_batch.cu:225-226).
+ * ====================================================================== */
+
+/* ppl0_batch_SpMM (include/dist_spmm_ppl_batch.cuh:202-245): local CSR chunks
+ * [local_row_lb, +local_row_num) and remote CSC chunks [remote_col_lb,
+ * +remote_col_num) of PE peid.  input = PE peid's X slice (symmetric
+ * convention above); remote rows are staged on chip by the kernel. */
+cola_status cola_ppl0_batch_spmm(float *output, const float *input, const int32_t *csr_rowPtr_l,
+                                 const int32_t *csr_colIdx_l, const int32_t *csr_rowIdx_zip_l,
+                                 const float *csr_val_l, const int32_t *csc_colPtr_r, const int32_t *csc_rowIdx_r,
+                                 const int32_t *csc_colIdx_zip_r, const float *csc_val_r, int32_t local_row_lb,
+                                 int32_t remote_col_lb, int32_t local_row_num, int32_t remote_col_num,
+                                 int32_t dim, int32_t nodesPerPE, int32_t peid, cola_stream_t stream);
+
+/* ppl0_batch_SpMM_seq (include/dist_spmm_ppl_batch.cuh:543-587): same result
+ * as cola_ppl0_batch_spmm (the reference's variant only orders work
+ * differently). */
+cola_status cola_ppl0_batch_spmm_seq(float *output, const float *input, const int32_t *csr_rowPtr_l,
+                                     const int32_t *csr_colIdx_l, const int32_t *csr_rowIdx_zip_l,
+                                     const float *csr_val_l, const int32_t *csc_colPtr_r,
+                                     const int32_t *csc_rowIdx_r, const int32_t *csc_colIdx_zip_r,
+                                     const float *csc_val_r, int32_t local_row_lb, int32_t remote_col_lb,
+                                     int32_t local_row_num, int32_t remote_col_num, int32_t dim,
+                                     int32_t nodesPerPE, int32_t peid, cola_stream_t stream);
+
+/* ppl0_batch_buffer_SpMM (include/dist_spmm_ppl_batch.cuh:373-417): remote
+ * rows are first gathered into comm_buffer (row j of comm_buffer = remote
+ * chunk j's column; it must hold remote_col_lb + remote_col_num rows of dim
+ * floats), in batches, then consumed from there. */
+cola_status cola_ppl0_batch_buffer_spmm(float *output, const float *input, float *comm_buffer,
+                                        const int32_t *csr_rowPtr_l, const int32_t *csr_colIdx_l,
+                                        const int32_t *csr_rowIdx_zip_l, const float *csr_val_l,
+                                        const int32_t *csc_colPtr_r, const int32_t *csc_rowIdx_r,
+                                        const int32_t *csc_colIdx_zip_r, const float *csc_val_r,
+                                        int32_t local_row_lb, int32_t remote_col_lb, int32_t local_row_num,
+                                        int32_t remote_col_num, int32_t dim, int32_t nodesPerPE, int32_t peid,
+                                        cola_stream_t stream);
+
+/* ppl_batch_SpMM (include/dist_spmm_ppl_batch.cuh:709-760): stage-i CSC
+ * scatter over remote chunks [remote_col_lb, remote_col_ub).  Chunks in
+ * [local_col_lb, local_col_ub) read row idx_ppl[w] of `input` (this PE's
+ * received pipeline buffer); the others read row idx_ppl[w] of group peer
+ * (col/npp) % group_size + group_offset's buffer (symmetric convention). */
+cola_status cola_ppl_batch_spmm(float *output, const float *input, const int32_t *csc_colPtr_r,
+                                const int32_t *csc_rowIdx_r, const int32_t *csc_colIdx_zip_r,
+                                const float *csc_val_r, int32_t local_col_lb, int32_t local_col_ub,
+                                int32_t remote_col_lb, int32_t remote_col_ub, int32_t stage,
+                                const int32_t *idx_ppl, int32_t dim, int32_t nodesPerPE, int32_t group_size,
+                                int32_t group_offset, int32_t peid, cola_stream_t stream);
+
+/* batching_data_ppl (include/dist_spmm_ppl_batch.cuh:59-73): the staged
+ * gather send[b,:] = input[put_colIdx[b] % nodesPerPE, :], b < nemb. */
+cola_status cola_batching_data_ppl(const float *input, float *send, const int32_t *put_colIdx, int32_t nemb,
+                                   int32_t dim, int32_t nodesPerPE, int32_t group_size, cola_stream_t stream);
+
+/* ========================================================================
+ * Graph-level API: device-resident partitions, all P virtual PEs in one call.
+ * Replaces distSpMM_ppl_batch / distSpMM_ppl_batch_wrapper
+ * (include/dist_spmm_ppl_batch.cuh:762-918) on one GPU.
+ * ====================================================================== */
+
+typedef struct cola_graph cola_graph;
+
+typedef struct cola_upload_opts {
+    int32_t if_split;    /* nnz_split the remote CSC too (src/distSpMM_ppl_batch.cu:86-98); 1 = yes */
+    int32_t group_size;  /* work-group size for the pipelined schedule; 0 or nparts = single stage */
+    int32_t reserved[6];
+} cola_upload_opts;
+
+/* Splits, builds stage tables and uploads every partition to the current
+ * device.  opts may be NULL (if_split = 1, group_size = nparts). */
+cola_status cola_graph_upload(const cola_partition_set *parts, const cola_upload_opts *opts, cola_graph **out,
+                              cola_stream_t stream);
+cola_status cola_graph_free(cola_graph *g);
+
+typedef struct cola_graph_info {
+    int32_t num_nodes, nparts, nodes_per_part, group_size;
+    int64_t nnz, nnz_local, nnz_remote;
+    int64_t local_chunks, remote_chunks, remote_cols;
+    int64_t device_bytes;
+} cola_graph_info;
+cola_status cola_graph_get_info(const cola_graph *g, cola_graph_info *out);
+
+/* Device pointers of partition `part`'s split arrays (the d_csr_zip / d_csc_zip
+ * members of include/sparse_data.h:28-77) and its chunk counts. */
+typedef struct cola_zip_view {
+    const int32_t *csr_rowPtr, *csr_colIdx, *csr_rowIdx_zip;
+    const float *csr_val;
+    const int32_t *csc_colPtr, *csc_rowIdx, *csc_colIdx_zip;
+    const float *csc_val;
+    int32_t local_chunks, remote_chunks;
+    int64_t nnz_l, nnz_r;
+} cola_zip_view;
+cola_status cola_graph_zip_view(const cola_graph *g, int32_t part, cola_zip_view *out);
+
+enum cola_schedule {
+    COLA_SCHEDULE_AUTO = 0,     /* pick by measurement / tuning cache */
+    COLA_SCHEDULE_FUSED = 1,    /* one launch: local CSR + remote CSC, rows staged on chip */
+    COLA_SCHEDULE_BUFFER = 2,   /* remote rows gathered into an HBM staging buffer in batches first */
+    COLA_SCHEDULE_PIPELINE = 3  /* the reference's multi-stage work-group schedule */
+};
+
+typedef struct cola_spmm_opts {
+    int32_t accumulate;         /* 0: Y is overwritten; 1: Y += A X (Y must be FP32) */
+    int32_t schedule;           /* enum cola_schedule */
+    int32_t gather_batch_rows;  /* staging batch (rows) for BUFFER/PIPELINE; 0 = 4096 */
+    int32_t reserved[5];
+} cola_spmm_opts;
+
+/* Y = A X (or Y += A X) for all partitions.  X: >= P*npp rows (rows past N are
+ * read only if the caller's X has them; padding rows are never referenced),
+ * ldx >= K elements; Y: N rows, ldy >= K.  x_dtype FP32 or BF16 (BF16 is
+ * widened exactly and accumulated in FP32); y_dtype FP32 or BF16 (rounded
+ * once, at the end).  opts may be NULL. */
+cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype x_dtype, int64_t ldx, void *Y, cola_dtype y_dtype,
+                      int64_t ldy, int32_t K, const cola_spmm_opts *opts, cola_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COLA_SPMM_H */

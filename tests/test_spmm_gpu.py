@@ -1,0 +1,340 @@
+"""GPU parity of the partitioned SpMM: every schedule and launcher against the
+FP64 oracle, and the kernel-level drop-ins against the reference's own CUDA
+kernels (oracle/_ref, compiled from the reference tree through the NVSHMEM
+shim) on the same seeded inputs.  Tolerances: FP32 paths 1e-5 relative
+Frobenius; BF16 storage 1e-2 against FP64 on the FP32 features."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import cola_b200 as cb
+from cola_b200 import spmm as S
+from oracle import oracle
+
+from gpu_util import TOL_BF16, TOL_F32, bf16_bits, dense_x, fp64_reference, graph_case, ptr, rel
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+
+
+@pytest.fixture(scope="module")
+def case12():
+    n, row, col, val, ps = graph_case(12, 16, seed=5, nparts=4)
+    return n, row, col, val, ps
+
+
+@pytest.mark.parametrize("K", [1, 3, 16, 32, 33, 64, 96, 100, 128, 256, 512])
+def test_fused_fp32_matches_fp64(case12, K):
+    n, row, col, val, ps = case12
+    g = S.Graph(ps)
+    X = dense_x(n, K, seed=K)
+    ref = fp64_reference(n, row, col, val, X)
+    Y = g.spmm(torch.from_numpy(X).to(DEV), schedule=S.SCHEDULE_FUSED)
+    torch.cuda.synchronize()
+    assert rel(Y.cpu().numpy(), ref) <= TOL_F32
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 8, 16])
+def test_partition_counts(P):
+    n, row, col, val, ps = graph_case(11, 12, seed=P, nparts=P)
+    g = S.Graph(ps)
+    X = dense_x(n, 64, seed=1)
+    ref = fp64_reference(n, row, col, val, X)
+    Y = g.spmm(torch.from_numpy(X).to(DEV))
+    torch.cuda.synchronize()
+    assert rel(Y.cpu().numpy(), ref) <= TOL_F32
+
+
+@pytest.mark.parametrize("if_split", [True, False])
+@pytest.mark.parametrize("schedule,batch", [(S.SCHEDULE_FUSED, 0), (S.SCHEDULE_BUFFER, 0),
+                                            (S.SCHEDULE_BUFFER, 64)])
+def test_schedules_fp32(case12, if_split, schedule, batch):
+    n, row, col, val, ps = case12
+    g = S.Graph(ps, if_split=if_split)
+    X = dense_x(n, 128, seed=2)
+    ref = fp64_reference(n, row, col, val, X)
+    Y = g.spmm(torch.from_numpy(X).to(DEV), schedule=schedule, gather_batch_rows=batch)
+    torch.cuda.synchronize()
+    assert rel(Y.cpu().numpy(), ref) <= TOL_F32
+
+
+@pytest.mark.parametrize("P,gs", [(4, 1), (4, 2), (8, 2), (8, 4)])
+@pytest.mark.parametrize("K", [32, 128])
+def test_pipelined_schedule(P, gs, K):
+    n, row, col, val, ps = graph_case(12, 16, seed=9, nparts=P)
+    g = S.Graph(ps, group_size=gs)
+    X = dense_x(n, K, seed=3)
+    ref = fp64_reference(n, row, col, val, X)
+    Y = g.spmm(torch.from_numpy(X).to(DEV), schedule=S.SCHEDULE_PIPELINE)
+    torch.cuda.synchronize()
+    assert rel(Y.cpu().numpy(), ref) <= TOL_F32
+
+
+@pytest.mark.parametrize("K", [64, 256])
+def test_bf16_storage(case12, K):
+    n, row, col, val, ps = case12
+    g = S.Graph(ps)
+    X = dense_x(n, K, seed=4)
+    Xb = bf16_bits(X)
+    ref_f32x = fp64_reference(n, row, col, val, X)
+    rp, ci, vv = oracle.global_csr(n, row, col, val)
+    ref_bf16x = oracle.spmm_csr_f64(rp, ci, vv, Xb)
+    xt = torch.from_numpy(Xb.view(np.int16)).view(torch.bfloat16).to(DEV)
+    Y32 = g.spmm(xt, out_dtype=torch.float32)
+    Y16 = g.spmm(xt, out_dtype=torch.bfloat16)
+    torch.cuda.synchronize()
+    y32 = Y32.cpu().numpy()
+    y16 = Y16.float().cpu().numpy()
+    # FP32 accumulation of exactly-widened BF16 features: FP32-level error
+    assert rel(y32, ref_bf16x) <= TOL_F32
+    # against FP64 on the FP32 features: BF16 storage error only
+    assert rel(y32, ref_f32x) <= TOL_BF16
+    assert rel(y16, ref_f32x) <= TOL_BF16
+    # BF16 output is the FP32 result rounded once
+    np.testing.assert_array_equal(Y16.cpu(), Y32.to(torch.bfloat16).cpu())
+
+
+def test_accumulate_and_strides(case12):
+    n, row, col, val, ps = case12
+    g = S.Graph(ps)
+    K = 64
+    X = dense_x(n, K, seed=6)
+    ref = fp64_reference(n, row, col, val, X)
+    big = torch.zeros((n, 80), device=DEV)
+    big[:, :K] = torch.from_numpy(X).to(DEV)
+    xv = big[:, :K]  # ldx = 80
+    Y = torch.zeros((n, 72), device=DEV)
+    yv = Y[:, :K]  # ldy = 72
+    g.spmm(xv, yv)
+    g.spmm(xv, yv, accumulate=True)
+    torch.cuda.synchronize()
+    assert rel(yv.cpu().numpy(), 2 * ref) <= TOL_F32
+    assert torch.all(Y[:, K:] == 0)
+
+
+def test_pipeline_and_buffer_bf16(case12):
+    n, row, col, val, _ = case12
+    ps = cb.PartitionSet.from_coo(n, row, col, val, 4)
+    g = S.Graph(ps, group_size=2)
+    X = dense_x(n, 128, seed=8)
+    rp, ci, vv = oracle.global_csr(n, row, col, val)
+    Xb = bf16_bits(X)
+    ref = oracle.spmm_csr_f64(rp, ci, vv, Xb)
+    xt = torch.from_numpy(Xb.view(np.int16)).view(torch.bfloat16).to(DEV)
+    for sch in (S.SCHEDULE_PIPELINE, S.SCHEDULE_BUFFER, S.SCHEDULE_FUSED):
+        Y = g.spmm(xt, schedule=sch, gather_batch_rows=100)
+        torch.cuda.synchronize()
+        assert rel(Y.cpu().numpy(), ref) <= TOL_F32, sch
+
+
+def test_golden_graphs_on_gpu():
+    from conftest import GOLDEN_CASES, load_golden
+    for name in GOLDEN_CASES:
+        fx = load_golden(name)
+        n = int(fx["num_nodes"])
+        rng = np.random.Generator(np.random.Philox(17))
+        val = rng.random(len(fx["row"]), dtype=np.float32)
+        for P in fx["nparts_list"]:
+            ps = cb.PartitionSet.from_coo(n, fx["row"], fx["col"], val, int(P))
+            g = S.Graph(ps)
+            X = dense_x(n, 32, seed=int(P))
+            ref = fp64_reference(n, fx["row"], fx["col"], val, X)
+            Y = g.spmm(torch.from_numpy(X).to(DEV))
+            torch.cuda.synchronize()
+            assert rel(Y.cpu().numpy(), ref) <= TOL_F32, (name, P)
+
+
+def test_empty_graph():
+    ps = cb.PartitionSet.from_coo(10, np.zeros(0, np.int32), np.zeros(0, np.int32), None, 4)
+    g = S.Graph(ps)
+    Y = g.spmm(torch.ones((10, 16), device=DEV))
+    torch.cuda.synchronize()
+    assert torch.all(Y == 0)
+
+
+def test_bad_arguments_raise(case12):
+    n, row, col, val, ps = case12
+    g = S.Graph(ps)
+    with pytest.raises(ValueError):
+        g.spmm(torch.ones((n - 1, 16), device=DEV))
+    with pytest.raises(cb.ColaError):
+        g.spmm(torch.ones((n, 16), device=DEV), torch.empty((n, 16), dtype=torch.bfloat16, device=DEV),
+               accumulate=True)
+    with pytest.raises(cb.ColaError):
+        g.spmm(torch.ones((n, 16), device=DEV), schedule=S.SCHEDULE_PIPELINE)
+    with pytest.raises(cb.ColaError):
+        S.Graph(ps, group_size=3)
+
+
+# ---------------------------------------------------------------------------
+# kernel-level drop-ins vs the reference's own kernels
+# ---------------------------------------------------------------------------
+def _padded_x(n, P, npp, K, seed):
+    X = np.zeros((P * npp, K), np.float32)
+    X[:n] = dense_x(n, K, seed)
+    return X
+
+
+def _run_dropin(fn, g, Xd, npp, K, P, buf=None):
+    Y = torch.zeros((P * npp, K), device=DEV)
+    for p in range(P):
+        z = g.zip_view(p)
+        args = [ptr(Y[p * npp:]), ptr(Xd[p * npp:])]
+        if buf is not None:
+            args.append(ptr(buf))
+        args += [z.csr_rowPtr, z.csr_colIdx, z.csr_rowIdx_zip, z.csr_val, z.csc_colPtr, z.csc_rowIdx,
+                 z.csc_colIdx_zip, z.csc_val]
+        args = [a if a is None or isinstance(a, ctypes.c_void_p) else ctypes.c_void_p(a) for a in args]
+        fn(*args, 0, 0, z.local_chunks, z.remote_chunks, K, npp, p, None)
+    torch.cuda.synchronize()
+    return Y
+
+
+def _run_reference(g, Xd, npp, K, P):
+    R = oracle.ref()
+    CF = (K + 31) // 32
+    res = 1 if K & 31 else 0
+    Y = torch.zeros((P * npp, K), device=DEV)
+    for p in range(P):
+        z = g.zip_view(p)
+        assert R.ref_set_pe(p, npp * K, None) == 0
+        rc = R.ref_ppl0_batch_spmm(CF, res, ptr(Y[p * npp:]), ptr(Xd[p * npp:]), z.csr_rowPtr, z.csr_colIdx,
+                                   z.csr_rowIdx_zip, z.csr_val, z.csc_colPtr, z.csc_rowIdx, z.csc_colIdx_zip,
+                                   z.csc_val, 0, 0, z.local_chunks, z.remote_chunks, K, npp, p, None)
+        assert rc == 0
+    torch.cuda.synchronize()
+    return Y
+
+
+needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built")
+
+
+@needs_ref
+@pytest.mark.parametrize("K", [16, 32, 64, 100, 128, 256])
+def test_ppl0_dropin_matches_reference_kernels(K):
+    P = 4
+    n, row, col, val, ps = graph_case(12, 16, seed=21, nparts=P)
+    g = S.Graph(ps)
+    npp = g.nodes_per_part
+    X = _padded_x(n, P, npp, K, seed=K)
+    Xd = torch.from_numpy(X).to(DEV)
+    ref64 = fp64_reference(n, row, col, val, X[:n])
+    L = cb.lib()
+    ours = _run_dropin(L.cola_ppl0_batch_spmm, g, Xd, npp, K, P)[:n].cpu().numpy()
+    theirs = _run_reference(g, Xd, npp, K, P)[:n].cpu().numpy()
+    assert rel(theirs, ref64) <= TOL_F32
+    assert rel(ours, ref64) <= TOL_F32
+    assert rel(ours, theirs) <= TOL_F32
+    seq = _run_dropin(L.cola_ppl0_batch_spmm_seq, g, Xd, npp, K, P)[:n].cpu().numpy()
+    assert rel(seq, theirs) <= TOL_F32
+    nr = max(g.zip_view(p).remote_chunks for p in range(P))
+    buf = torch.empty((max(nr, 1), K), device=DEV)
+    bufd = _run_dropin(L.cola_ppl0_batch_buffer_spmm, g, Xd, npp, K, P, buf=buf)[:n].cpu().numpy()
+    assert rel(bufd, theirs) <= TOL_F32
+
+
+def _pipeline_tables(n, row, col, ps, P, gs):
+    wg = [cb.workgroup_cols(n, row, col, P, gs, s) for s in range(P // gs)]
+    tabs = []
+    for me in range(P):
+        p = ps.part(me)
+        lt, lp = cb.nnz_split(p["csr_rowIdx_l"], p["csr_rowPtr_l"], len(p["csr_colIdx_l"]))
+        rt, rp = cb.nnz_split(p["csc_colIdx_r"], p["csc_colPtr_r"], len(p["csc_rowIdx_r"]))
+        tabs.append(oracle.stage_tables(me, P, gs, n, rt, len(lt), wg))
+    return tabs
+
+
+@needs_ref
+@pytest.mark.parametrize("P,gs", [(4, 1), (4, 2), (8, 2)])
+def test_pipelined_dropins_match_reference_kernels(P, gs):
+    """The multi-stage schedule of include/dist_spmm_ppl_batch.cuh:785-836 run
+    in lockstep over P virtual PEs, once with the reference's kernels and once
+    with the drop-ins, on the oracle's stage tables."""
+    K = 64
+    n, row, col, val, ps = graph_case(12, 16, seed=31, nparts=P)
+    g = S.Graph(ps)
+    npp = g.nodes_per_part
+    X = _padded_x(n, P, npp, K, seed=5)
+    Xd = torch.from_numpy(X).to(DEV)
+    ref64 = fp64_reference(n, row, col, val, X[:n])
+    tabs = _pipeline_tables(n, row, col, ps, P, gs)
+    nstages = P // gs
+    R = oracle.ref()
+    L = cb.lib()
+    CF, res = (K + 31) // 32, 1 if K & 31 else 0
+    results = {}
+    for impl in ("ref", "ours"):
+        Y = torch.zeros((P * npp, K), device=DEV)
+        bufs = [torch.zeros((P * npp, K), device=DEV) for _ in range(2)]
+        send = torch.zeros((P * npp, K), device=DEV)
+        dev_idx = [[torch.from_numpy(t["idx_ppl"][i]).to(DEV) for i in range(nstages - 1)] for t in tabs]
+        dev_put = [[torch.from_numpy(t["put_colIdx"][i]).to(DEV) for i in range(nstages - 1)] for t in tabs]
+        # stage 0 for every PE (dist_spmm_ppl_batch.cuh:797-805)
+        for me in range(P):
+            z = g.zip_view(me)
+            t = tabs[me]
+            lo, ro = t["local_offset"], t["remote_offset"]
+            args = (ptr(Y[me * npp:]), ptr(Xd[me * npp:]), z.csr_rowPtr, z.csr_colIdx, z.csr_rowIdx_zip, z.csr_val,
+                    z.csc_colPtr, z.csc_rowIdx, z.csc_colIdx_zip, z.csc_val, int(lo[0]), int(ro[0]),
+                    int(lo[1] - lo[0]), int(ro[1] - ro[0]), K, npp, me, None)
+            if impl == "ref":
+                assert R.ref_set_pe(me, npp * K, None) == 0
+                assert R.ref_ppl0_batch_spmm(CF, res, *args) == 0
+            else:
+                cb._lib.check(L.cola_ppl0_batch_spmm(*args))
+        for i in range(1, nstages):
+            buf = bufs[(i - 1) % 2]
+            # every PE's put for stage i (:788-793, :811-816)
+            for me in range(P):
+                t = tabs[me]
+                target = ((me - i * gs) % P + P) % P
+                nemb = int(t["put_offset"][2 * (i - 1) + 1] - t["put_offset"][2 * (i - 1)])
+                if nemb == 0:
+                    continue
+                if impl == "ref":
+                    assert R.ref_set_pe(me, npp * K, None) == 0
+                    assert R.ref_batching_data_ppl(ptr(Xd[me * npp:]), ptr(send[me * npp:]), ptr(dev_put[me][i - 1]),
+                                                   nemb, K, npp, gs, None) == 0
+                else:
+                    cb._lib.check(L.cola_batching_data_ppl(ptr(Xd[me * npp:]), ptr(send[me * npp:]),
+                                                           ptr(dev_put[me][i - 1]), nemb, K, npp, gs, None))
+                buf[target * npp: target * npp + nemb].copy_(send[me * npp: me * npp + nemb])
+            # every PE's stage-i compute (:822-835)
+            for me in range(P):
+                z = g.zip_view(me)
+                t = tabs[me]
+                lo, ro = t["local_offset"], t["remote_offset"]
+                if ro[2 * i + 1] - ro[2 * i] == 0:
+                    continue
+                args = (ptr(Y[me * npp:]), ptr(buf[me * npp:]), z.csc_colPtr, z.csc_rowIdx, z.csc_colIdx_zip,
+                        z.csc_val, int(lo[2 * i]), int(lo[2 * i + 1]), int(ro[2 * i]), int(ro[2 * i + 1]), i,
+                        ptr(dev_idx[me][i - 1]), K, npp, gs, me // gs * gs, me, None)
+                if impl == "ref":
+                    assert R.ref_set_pe(me, npp * K, None) == 0
+                    assert R.ref_ppl_batch_spmm(CF, res, *args) == 0
+                else:
+                    cb._lib.check(L.cola_ppl_batch_spmm(*args))
+        torch.cuda.synchronize()
+        results[impl] = Y[:n].cpu().numpy()
+    assert rel(results["ref"], ref64) <= TOL_F32  # pins the stage tables' meaning
+    assert rel(results["ours"], ref64) <= TOL_F32
+    assert rel(results["ours"], results["ref"]) <= TOL_F32
+
+
+@needs_ref
+def test_batching_data_ppl_matches_reference_bit_exact():
+    K, npp, P = 96, 500, 4
+    X = torch.from_numpy(dense_x(P * npp, K, seed=12)).to(DEV)
+    rng = np.random.Generator(np.random.Philox(3))
+    idx = torch.from_numpy(rng.integers(0, P * npp, 700).astype(np.int32)).to(DEV)
+    a = torch.zeros((700, K), device=DEV)
+    b = torch.zeros((700, K), device=DEV)
+    R = oracle.ref()
+    assert R.ref_set_pe(0, npp * K, None) == 0
+    assert R.ref_batching_data_ppl(ptr(X), ptr(a), ptr(idx), 700, K, npp, 1, None) == 0
+    cb._lib.check(cb.lib().cola_batching_data_ppl(ptr(X), ptr(b), ptr(idx), 700, K, npp, 1, None))
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
