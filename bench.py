@@ -314,26 +314,28 @@ def run_ours(args, w):
     del Yacc
 
     # end to end through the public API: pinned host X -> device, SpMM, Y -> pinned host
-    Xpin = torch.from_numpy(Xh).to(xdt).pin_memory()
-    Ypin = torch.empty((n, K), dtype=ydt).pin_memory()
-    Xe = torch.empty_like(X)
-    e2e_steps = max(1, min(args.steps, 10))
-    for _ in range(2):
-        Xe.copy_(Xpin, non_blocking=True)
-        g.spmm(Xe, Y, schedule=sched, stream=stream)
-        Ypin.copy_(Y, non_blocking=True)
-    torch.cuda.synchronize()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        Xe.copy_(Xpin, non_blocking=True)
-        g.spmm(Xe, Y, schedule=sched, stream=stream)
-        Ypin.copy_(Y, non_blocking=True)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
-    barrier()
+    e2e_ms = None
+    if not args.no_e2e:
+        Xpin = torch.from_numpy(Xh).to(xdt).pin_memory()
+        Ypin = torch.empty((n, K), dtype=ydt).pin_memory()
+        Xe = torch.empty_like(X)
+        e2e_steps = max(1, min(args.steps, 10))
+        for _ in range(2):
+            Xe.copy_(Xpin, non_blocking=True)
+            g.spmm(Xe, Y, schedule=sched, stream=stream)
+            Ypin.copy_(Y, non_blocking=True)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            Xe.copy_(Xpin, non_blocking=True)
+            g.spmm(Xe, Y, schedule=sched, stream=stream)
+            Ypin.copy_(Y, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
+        barrier()
 
     peak, peak_kind = measured_peak()
     achieved = B / (k_ms * 1e-3) / 1e9
@@ -355,8 +357,9 @@ def run_ours(args, w):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
                      "kernel_ms": k_ms, "frac_of_8TBs": achieved / 8000.0},
-        "e2e": {"value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": n * K * s_x,
-                "d2h_bytes_per_step": n * K * s_y, "ms_per_step": e2e_ms},
+        "e2e": None if e2e_ms is None else {
+            "value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": n * K * s_x,
+            "d2h_bytes_per_step": n * K * s_y, "ms_per_step": e2e_ms},
         "gpu_launches": (launches_per_step * args.steps) if launches_per_step else None,
         "clocks": clk,
     }
@@ -392,8 +395,13 @@ def main():
     ap.add_argument("--workload", default="fp32", choices=sorted(WORKLOADS))
     ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "buffer"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
     args = ap.parse_args()
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.scale is not None:
+        w["scale"] = args.scale
+        w["desc"] = "{} [scale overridden to {}]".format(w["desc"], args.scale)
     if args.impl == "reference":
         return run_reference(args, w)
     return run_ours(args, w)

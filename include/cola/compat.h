@@ -1,0 +1,311 @@
+/*
+ * cola/compat.h -- the reference's C++ surface (include/sparse_data.h and
+ * include/dist_spmm_ppl_batch.cuh of zzzlxhhh/CoLa) on top of the cola_b200 C
+ * ABI, so a caller written against those headers builds unchanged for one B200
+ * with P virtual PEs.  Header-only host C++; link libcola_b200.so and cudart.
+ *
+ * Differences a caller sees:
+ *  - errors throw cola_compat::error instead of calling exit();
+ *  - the device holders cannot be copied (the reference's can, and then double
+ *    free their memory);
+ *  - CF / is_residue template arguments are accepted and ignored: the library
+ *    dispatches on dim itself, for every dim >= 1 (the reference's wrapper
+ *    launches nothing for dim 65-96 or dim > 128);
+ *  - "symmetric" buffers (X slices, pipeline buffers) of the P virtual PEs must
+ *    be laid out back to back, nodesPerPE*dim floats apart, in one allocation
+ *    (see cola_spmm.h); NVSHMEM puts/gets become reads of that memory.
+ *  - the multi-stage schedule (group_size < nranks) runs all PEs together:
+ *    distSpMM_ppl_batch_all().  The per-PE wrapper supports group_size == nranks,
+ *    which is what P virtual partitions on one GPU map to.
+ */
+#ifndef COLA_COMPAT_H
+#define COLA_COMPAT_H
+
+#include <cuda_runtime_api.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../cola_spmm.h"
+
+namespace cola_compat {
+
+struct error : std::runtime_error {
+    cola_status status;
+    error(cola_status s, const std::string &what) : std::runtime_error(what), status(s) {}
+};
+
+inline void check(cola_status s, const char *where)
+{
+    if (s != COLA_SUCCESS)
+        throw error(s, std::string(where) + ": " + cola_status_string(s) + ": " + cola_last_error());
+}
+
+inline void check_cuda(cudaError_t e, const char *where)
+{
+    if (e != cudaSuccess)
+        throw error(COLA_ERROR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+inline T *upload(const std::vector<T> &v, const char *where)
+{
+    T *p = nullptr;
+    check_cuda(cudaMalloc((void **)&p, v.size() * sizeof(T)), where);
+    if (!v.empty())
+        check_cuda(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), where);
+    return p;
+}
+
+}  // namespace cola_compat
+
+/* include/sparse_data.h:6-27 */
+struct d_csr {
+    int *d_csr_rowPtr = nullptr;
+    int *d_csr_colIdx = nullptr;
+    float *d_csr_val = nullptr;
+    d_csr(std::vector<int> rowPtr, std::vector<int> colIdx, std::vector<float> val)
+    {
+        d_csr_rowPtr = cola_compat::upload(rowPtr, "d_csr");
+        d_csr_colIdx = cola_compat::upload(colIdx, "d_csr");
+        d_csr_val = cola_compat::upload(val, "d_csr");
+    }
+    d_csr(const d_csr &) = delete;
+    d_csr &operator=(const d_csr &) = delete;
+    ~d_csr()
+    {
+        cudaFree(d_csr_rowPtr);
+        cudaFree(d_csr_colIdx);
+        cudaFree(d_csr_val);
+    }
+};
+
+/* include/sparse_data.h:28-52 */
+struct d_csc_zip {
+    int *d_csc_colPtr = nullptr;
+    int *d_csc_rowIdx = nullptr;
+    int *d_csc_colIdx_zip = nullptr;
+    float *d_csc_val = nullptr;
+    d_csc_zip(std::vector<int> colPtr, std::vector<int> rowIdx, std::vector<int> colIdx_zip, std::vector<float> val)
+    {
+        d_csc_colPtr = cola_compat::upload(colPtr, "d_csc_zip");
+        d_csc_rowIdx = cola_compat::upload(rowIdx, "d_csc_zip");
+        d_csc_colIdx_zip = cola_compat::upload(colIdx_zip, "d_csc_zip");
+        d_csc_val = cola_compat::upload(val, "d_csc_zip");
+    }
+    d_csc_zip(const d_csc_zip &) = delete;
+    d_csc_zip &operator=(const d_csc_zip &) = delete;
+    ~d_csc_zip()
+    {
+        cudaFree(d_csc_colPtr);
+        cudaFree(d_csc_rowIdx);
+        cudaFree(d_csc_colIdx_zip);
+        cudaFree(d_csc_val);
+    }
+};
+
+/* include/sparse_data.h:54-77 */
+struct d_csr_zip {
+    int *d_csr_rowPtr = nullptr;
+    int *d_csr_colIdx = nullptr;
+    int *d_csr_rowIdx_zip = nullptr;
+    float *d_csr_val = nullptr;
+    d_csr_zip(std::vector<int> rowPtr, std::vector<int> colIdx, std::vector<int> rowIdx_zip, std::vector<float> val)
+    {
+        d_csr_rowPtr = cola_compat::upload(rowPtr, "d_csr_zip");
+        d_csr_colIdx = cola_compat::upload(colIdx, "d_csr_zip");
+        d_csr_rowIdx_zip = cola_compat::upload(rowIdx_zip, "d_csr_zip");
+        d_csr_val = cola_compat::upload(val, "d_csr_zip");
+    }
+    d_csr_zip(const d_csr_zip &) = delete;
+    d_csr_zip &operator=(const d_csr_zip &) = delete;
+    ~d_csr_zip()
+    {
+        cudaFree(d_csr_rowPtr);
+        cudaFree(d_csr_colIdx);
+        cudaFree(d_csr_rowIdx_zip);
+        cudaFree(d_csr_val);
+    }
+};
+
+/* include/dist_spmm_ppl_batch.cuh:7-27 (64-bit sizes; throws instead of exit) */
+template <typename T>
+std::vector<T> bin2vec(const std::string filename)
+{
+    static_assert(sizeof(T) == 4, "bin2vec: 4-byte element types only");
+    int64_t n = 0;
+    cola_compat::check(cola_bin_read_i32(filename.c_str(), nullptr, 0, &n), "bin2vec");
+    std::vector<T> v((size_t)n);
+    cola_compat::check(cola_bin_read_i32(filename.c_str(), reinterpret_cast<int32_t *>(v.data()), n, &n),
+                       "bin2vec");
+    return v;
+}
+
+/* include/dist_spmm_ppl_batch.cuh:29-56 */
+inline void nnz_split(std::vector<int> &rowIdx, std::vector<int> &rowPtr, std::vector<int> &colIdx,
+                      std::vector<int> &target, std::vector<int> &ptr, const int peid, bool local)
+{
+    int64_t n = 0;
+    cola_compat::check(cola_nnz_split(rowIdx.data(), (int64_t)rowIdx.size(), rowPtr.data(), (int64_t)colIdx.size(),
+                                      nullptr, nullptr, 0, &n),
+                       "nnz_split");
+    size_t t0 = target.size(), p0 = ptr.size();
+    target.resize(t0 + (size_t)n);
+    ptr.resize(p0 + (rowIdx.empty() ? 0 : (size_t)n + 1));
+    if (!rowIdx.empty())
+        cola_compat::check(cola_nnz_split(rowIdx.data(), (int64_t)rowIdx.size(), rowPtr.data(),
+                                          (int64_t)colIdx.size(), target.data() + t0, ptr.data() + p0, n, &n),
+                           "nnz_split");
+    if (!rowIdx.empty())
+        printf("PE-%d, %s_split_ratio:%.3f \n", peid, local ? "l" : "r", (float)n / rowIdx.size());
+}
+
+/* include/dist_spmm_ppl_batch.cuh:59-73 as a host call (launch shape is the library's) */
+inline void batching_data_ppl(const float *input_nvsh, float *ppl_send_nvsh, int *put_colIdx, const int nemb,
+                              const int dim, const int nodesPerPE, const int group_size, cudaStream_t stream)
+{
+    cola_compat::check(cola_batching_data_ppl(input_nvsh, ppl_send_nvsh, put_colIdx, nemb, dim, nodesPerPE,
+                                              group_size, (cola_stream_t)stream),
+                       "batching_data_ppl");
+}
+
+/* include/dist_spmm_ppl_batch.cuh:202-245 */
+template <int CF, bool is_residue>
+void ppl0_batch_SpMM(float *output, const float *input, const int *csr_rowPtr_l, const int *csr_colIdx_l,
+                     const int *csr_rowIdx_zip_l, const float *csr_val_l, const int *csc_colPtr_r,
+                     const int *csc_rowIdx_r, const int *csc_colIdx_zip_r, const float *csc_val_r,
+                     const int local_row_lb, const int remote_col_lb, const int local_row_num,
+                     const int remote_col_num, const int dim, const int nodesPerPE, const int peid,
+                     cudaStream_t stream)
+{
+    cola_compat::check(cola_ppl0_batch_spmm(output, input, csr_rowPtr_l, csr_colIdx_l, csr_rowIdx_zip_l, csr_val_l,
+                                            csc_colPtr_r, csc_rowIdx_r, csc_colIdx_zip_r, csc_val_r, local_row_lb,
+                                            remote_col_lb, local_row_num, remote_col_num, dim, nodesPerPE, peid,
+                                            (cola_stream_t)stream),
+                       "ppl0_batch_SpMM");
+}
+
+/* include/dist_spmm_ppl_batch.cuh:543-587 */
+template <int CF, bool is_residue>
+void ppl0_batch_SpMM_seq(float *output, const float *input, const int *csr_rowPtr_l, const int *csr_colIdx_l,
+                         const int *csr_rowIdx_zip_l, const float *csr_val_l, const int *csc_colPtr_r,
+                         const int *csc_rowIdx_r, const int *csc_colIdx_zip_r, const float *csc_val_r,
+                         const int local_row_lb, const int remote_col_lb, const int local_row_num,
+                         const int remote_col_num, const int dim, const int nodesPerPE, const int peid,
+                         cudaStream_t stream)
+{
+    cola_compat::check(cola_ppl0_batch_spmm_seq(output, input, csr_rowPtr_l, csr_colIdx_l, csr_rowIdx_zip_l,
+                                                csr_val_l, csc_colPtr_r, csc_rowIdx_r, csc_colIdx_zip_r, csc_val_r,
+                                                local_row_lb, remote_col_lb, local_row_num, remote_col_num, dim,
+                                                nodesPerPE, peid, (cola_stream_t)stream),
+                       "ppl0_batch_SpMM_seq");
+}
+
+/* include/dist_spmm_ppl_batch.cuh:373-417 */
+template <int CF, bool is_residue>
+void ppl0_batch_buffer_SpMM(float *output, const float *input, const float *comm_buffer, const int *csr_rowPtr_l,
+                            const int *csr_colIdx_l, const int *csr_rowIdx_zip_l, const float *csr_val_l,
+                            const int *csc_colPtr_r, const int *csc_rowIdx_r, const int *csc_colIdx_zip_r,
+                            const float *csc_val_r, const int local_row_lb, const int remote_col_lb,
+                            const int local_row_num, const int remote_col_num, const int dim, const int nodesPerPE,
+                            const int peid, cudaStream_t stream)
+{
+    cola_compat::check(cola_ppl0_batch_buffer_spmm(output, input, const_cast<float *>(comm_buffer), csr_rowPtr_l,
+                                                   csr_colIdx_l, csr_rowIdx_zip_l, csr_val_l, csc_colPtr_r,
+                                                   csc_rowIdx_r, csc_colIdx_zip_r, csc_val_r, local_row_lb,
+                                                   remote_col_lb, local_row_num, remote_col_num, dim, nodesPerPE,
+                                                   peid, (cola_stream_t)stream),
+                       "ppl0_batch_buffer_SpMM");
+}
+
+/* include/dist_spmm_ppl_batch.cuh:709-760 */
+template <int CF, bool is_residue>
+void ppl_batch_SpMM(float *output, const float *input, const int *csc_colPtr_r, const int *csc_rowIdx_r,
+                    const int *csc_colIdx_zip_r, const float *csc_val_r, const int local_col_lb,
+                    const int local_col_ub, const int remote_col_lb, const int remote_col_ub, const int stage,
+                    const int *idx_ppl, const int dim, const int nodesPerPE, const int group_size,
+                    const int group_offset, const int peid, cudaStream_t stream)
+{
+    cola_compat::check(cola_ppl_batch_spmm(output, input, csc_colPtr_r, csc_rowIdx_r, csc_colIdx_zip_r, csc_val_r,
+                                           local_col_lb, local_col_ub, remote_col_lb, remote_col_ub, stage, idx_ppl,
+                                           dim, nodesPerPE, group_size, group_offset, peid, (cola_stream_t)stream),
+                       "ppl_batch_SpMM");
+}
+
+/* include/dist_spmm_ppl_batch.cuh:851-918, one virtual PE, single stage.
+ * The reference routes group_size == nranks > 8 through the buffer kernel with
+ * CF = 1 (:872-883); here that case runs the same fused kernel (the result is
+ * the same; comm_buffer is not needed). */
+inline void distSpMM_ppl_batch_wrapper(const int group_size, float *output, const float *input_nvsh,
+                                       float **ppl_buffer_nvsh, float *ppl_send_nvsh, float *comm_buffer_nvsh,
+                                       int *local_offset_ppl, int *remote_offset_ppl, int *put_offset_ppl,
+                                       int **put_colIdx_ppl, int **idx_ppl, d_csr_zip *csr_zip_l,
+                                       d_csc_zip *csc_zip_r, const int block_lb, const int block_ub, const int dim,
+                                       const int nodesPerPE, const int nranks, const int mype_node,
+                                       cudaStream_t stream)
+{
+    (void)ppl_buffer_nvsh;
+    (void)ppl_send_nvsh;
+    (void)comm_buffer_nvsh;
+    (void)put_offset_ppl;
+    (void)put_colIdx_ppl;
+    (void)idx_ppl;
+    (void)block_lb;
+    (void)block_ub;
+    if (group_size != nranks)
+        throw cola_compat::error(COLA_ERROR_UNSUPPORTED,
+                                 "distSpMM_ppl_batch_wrapper: on one GPU the multi-stage schedule runs all virtual PEs "
+                                 "together; call distSpMM_ppl_batch_all()");
+    ppl0_batch_SpMM<1, false>(output, input_nvsh, csr_zip_l->d_csr_rowPtr, csr_zip_l->d_csr_colIdx,
+                              csr_zip_l->d_csr_rowIdx_zip, csr_zip_l->d_csr_val, csc_zip_r->d_csc_colPtr,
+                              csc_zip_r->d_csc_rowIdx, csc_zip_r->d_csc_colIdx_zip, csc_zip_r->d_csc_val,
+                              local_offset_ppl[0], remote_offset_ppl[0], local_offset_ppl[1] - local_offset_ppl[0],
+                              remote_offset_ppl[1] - remote_offset_ppl[0], dim, nodesPerPE, mype_node, stream);
+}
+
+/* The multi-stage schedule of include/dist_spmm_ppl_batch.cuh:785-836 for all
+ * nranks virtual PEs at once, in lockstep: stage 0 of every PE, then per stage
+ * i >= 1 every PE's put (a staged gather straight into the target PE's
+ * pipeline buffer) followed by every PE's stage-i compute.  Arrays are indexed
+ * by PE: offsets[pe] are the per-PE host tables of src/distSpMM_ppl_batch.cu,
+ * put_colIdx_ppl[pe][i] / idx_ppl[pe][i] device lists.  input_nvsh and
+ * output point at PE 0's slices; ppl_buffer_nvsh[0..1] at PE 0's copies of the
+ * two pipeline buffers (each holds nranks*nodesPerPE*dim floats). */
+inline void distSpMM_ppl_batch_all(const int group_size, float *output, const float *input_nvsh,
+                                   float **ppl_buffer_nvsh, int **local_offset_ppl, int **remote_offset_ppl,
+                                   int **put_offset_ppl, int ***put_colIdx_ppl, int ***idx_ppl,
+                                   d_csr_zip **csr_zip_l, d_csc_zip **csc_zip_r, const int dim, const int nodesPerPE,
+                                   const int nranks, cudaStream_t stream)
+{
+    const int nstages = nranks / group_size;
+    const long long pe = (long long)nodesPerPE * dim;
+    for (int me = 0; me < nranks; me++)
+        ppl0_batch_SpMM<1, false>(output + me * pe, input_nvsh + me * pe, csr_zip_l[me]->d_csr_rowPtr,
+                                  csr_zip_l[me]->d_csr_colIdx, csr_zip_l[me]->d_csr_rowIdx_zip,
+                                  csr_zip_l[me]->d_csr_val, csc_zip_r[me]->d_csc_colPtr, csc_zip_r[me]->d_csc_rowIdx,
+                                  csc_zip_r[me]->d_csc_colIdx_zip, csc_zip_r[me]->d_csc_val,
+                                  local_offset_ppl[me][0], remote_offset_ppl[me][0],
+                                  local_offset_ppl[me][1] - local_offset_ppl[me][0],
+                                  remote_offset_ppl[me][1] - remote_offset_ppl[me][0], dim, nodesPerPE, me, stream);
+    for (int i = 1; i < nstages; i++) {
+        float *buf = ppl_buffer_nvsh[(i - 1) % 2];
+        for (int me = 0; me < nranks; me++) {
+            const int target = ((me - i * group_size) % nranks + nranks) % nranks;
+            const int nemb = put_offset_ppl[me][2 * (i - 1) + 1] - put_offset_ppl[me][2 * (i - 1)];
+            batching_data_ppl(input_nvsh + me * pe, buf + target * pe, put_colIdx_ppl[me][i - 1], nemb, dim,
+                              nodesPerPE, group_size, stream);
+        }
+        for (int me = 0; me < nranks; me++)
+            ppl_batch_SpMM<1, false>(output + me * pe, buf + me * pe, csc_zip_r[me]->d_csc_colPtr,
+                                     csc_zip_r[me]->d_csc_rowIdx, csc_zip_r[me]->d_csc_colIdx_zip,
+                                     csc_zip_r[me]->d_csc_val, local_offset_ppl[me][2 * i],
+                                     local_offset_ppl[me][2 * i + 1], remote_offset_ppl[me][2 * i],
+                                     remote_offset_ppl[me][2 * i + 1], i, idx_ppl[me][i - 1], dim, nodesPerPE,
+                                     group_size, me / group_size * group_size, me, stream);
+    }
+}
+
+#endif /* COLA_COMPAT_H */
