@@ -5,7 +5,8 @@
 Default workload: R-MAT scale 20 (1,048,576 nodes), avg degree 32, symmetrised,
 values D^-1/2 A D^-1/2, P = 8 virtual row partitions, X 1,048,576 x 128 FP32
 ~N(0,1) (Philox, seed 2), FP32 output.  A step is one Y = A X over all
-partitions (Y zeroed, then one fused launch), inputs resident in HBM.  The
+partitions, inputs resident in HBM (default schedule: the row-major view, one
+writer per output row; --schedule fused runs the CSC-scatter kernel).  The
 metric is algorithmic HBM GB/s:
     B = nnz*(4 + s_v + K*s_x) + (M+1)*4 + M*K*s_y   (s_v = 4)
 per step divided by the step time.  Inputs (X 512 MiB, Y 512 MiB) are larger
@@ -257,7 +258,8 @@ def run_ours(args, w):
     Xh = dense_x(n, K, w["seed"])
     t_prep = time.time() - t0
     stream = torch.cuda.current_stream()
-    g = S.Graph(ps, stream=stream)
+    g = S.Graph(ps, hub_threshold=args.hub_threshold, hub_segment=args.hub_segment, task_entries=args.task_entries,
+                stream=stream)
     info = g.info
     xdt = torch.float32 if w["xdt"] == "fp32" else torch.bfloat16
     ydt = torch.float32 if w["ydt"] == "fp32" else torch.bfloat16
@@ -265,11 +267,13 @@ def run_ours(args, w):
     s_y = 4 if ydt == torch.float32 else 2
     X = torch.from_numpy(Xh).to(dev).to(xdt)
     Y = torch.empty((n, K), dtype=ydt, device=dev)
-    sched = {"auto": S.SCHEDULE_AUTO, "fused": S.SCHEDULE_FUSED, "buffer": S.SCHEDULE_BUFFER}[args.schedule]
+    sched = {"auto": S.SCHEDULE_AUTO, "fused": S.SCHEDULE_FUSED, "buffer": S.SCHEDULE_BUFFER,
+             "rows": S.SCHEDULE_ROWS}[args.schedule]
+    eff = S.SCHEDULE_ROWS if sched == S.SCHEDULE_AUTO else sched
     B = alg_bytes(int(info.nnz), n, K, s_x, s_y)
 
     def step():
-        g.spmm(X, Y, schedule=sched, stream=stream)
+        g.spmm(X, Y, schedule=sched, unroll=args.unroll, min_blocks=args.min_blocks, stream=stream)
 
     def barrier():
         if world > 1:
@@ -300,12 +304,13 @@ def run_ours(args, w):
     ms = ev[0].elapsed_time(ev[1]) / args.steps
     ms = max_over_ranks(ms)
 
-    # dominant kernel alone (accumulate mode: the same fused launch, no zeroing)
-    Yacc = torch.zeros((n, K), dtype=torch.float32, device=dev)
+    # the SpMM kernels alone: for the fused schedule in accumulate mode (the same
+    # launch without the Y zeroing); the row-major schedule has no zeroing
+    Yacc = torch.zeros((n, K), dtype=torch.float32, device=dev) if eff == S.SCHEDULE_FUSED else Y
     kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     for a, b in kev:
         a.record(stream)
-        g.spmm(X, Yacc, accumulate=True, schedule=sched, stream=stream)
+        g.spmm(X, Yacc, accumulate=(eff == S.SCHEDULE_FUSED), schedule=sched, unroll=args.unroll, min_blocks=args.min_blocks, stream=stream)
         b.record(stream)
     torch.cuda.synchronize()
     k_ms = sum(a.elapsed_time(b) for a, b in kev) / len(kev)
@@ -341,7 +346,12 @@ def run_ours(args, w):
     achieved = B / (k_ms * 1e-3) / 1e9
     traffic = read_traffic("fused_spmm_rmat20_k128_fp32.txt") if args.workload == "fp32" else \
         read_traffic("fused_spmm_rmat21_k256_bf16.txt")
-    launches_per_step = 1 if sched in (S.SCHEDULE_AUTO, S.SCHEDULE_FUSED) else None
+    if eff == S.SCHEDULE_ROWS:
+        launches_per_step = 1 + (1 if info.hub_rows > 0 else 0)
+    elif eff == S.SCHEDULE_FUSED:
+        launches_per_step = 1
+    else:
+        launches_per_step = None
     line = {
         "metric": METRIC, "value": B * world / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -350,7 +360,11 @@ def run_ours(args, w):
         "config": {"workload": w["desc"], "nodes": n, "nnz": int(info.nnz), "nnz_local": int(info.nnz_local),
                    "nnz_remote": int(info.nnz_remote), "K": K, "nparts": w["P"], "local_chunks": int(info.local_chunks),
                    "remote_chunks": int(info.remote_chunks), "parallelism": "replicas x{}".format(world),
-                   "schedule": args.schedule, "alg_bytes_per_step": B,
+                   "schedule": {S.SCHEDULE_ROWS: "rows", S.SCHEDULE_FUSED: "fused",
+                                S.SCHEDULE_BUFFER: "buffer"}.get(eff, args.schedule),
+                   "hub_rows": int(info.hub_rows), "hub_segments": int(info.hub_segments),
+                   "unroll": args.unroll or 4, "row_tasks": int(info.row_tasks),
+                   "alg_bytes_per_step": B,
                    "l2": "inputs larger than L2 (X {:.0f} MiB, Y {:.0f} MiB); no flush".format(
                        n * K * s_x / 2 ** 20, n * K * s_y / 2 ** 20),
                    "prep_seconds": round(t_prep, 1)},
@@ -393,9 +407,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="fp32", choices=sorted(WORKLOADS))
-    ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "buffer"])
+    ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "buffer", "rows"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--hub-threshold", type=int, default=0, help="row-major schedule: hub split threshold")
+    ap.add_argument("--hub-segment", type=int, default=0, help="row-major schedule: hub segment length")
+    ap.add_argument("--unroll", type=int, default=0, help="row-major schedule: loads in flight per lane group")
+    ap.add_argument("--task-entries", type=int, default=0, help="row-major schedule: entries per row-block task")
+    ap.add_argument("--min-blocks", type=int, default=0, help="row-major schedule: resident blocks per SM")
     ap.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
     args = ap.parse_args()
     w = dict(WORKLOADS[args.workload])

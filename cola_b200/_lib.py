@@ -25,6 +25,7 @@ SCHEDULE_AUTO = 0
 SCHEDULE_FUSED = 1
 SCHEDULE_BUFFER = 2
 SCHEDULE_PIPELINE = 3
+SCHEDULE_ROWS = 4
 
 
 class ColaError(RuntimeError):
@@ -43,13 +44,15 @@ class PartitionView(ctypes.Structure):
 
 
 class UploadOpts(ctypes.Structure):
-    _fields_ = [("if_split", I32), ("group_size", I32), ("reserved", I32 * 6)]
+    _fields_ = [("if_split", I32), ("group_size", I32), ("no_row_view", I32), ("hub_threshold", I32),
+                ("hub_segment", I32), ("task_entries", I32), ("reserved", I32 * 2)]
 
 
 class GraphInfo(ctypes.Structure):
     _fields_ = [("num_nodes", I32), ("nparts", I32), ("nodes_per_part", I32), ("group_size", I32),
                 ("nnz", I64), ("nnz_local", I64), ("nnz_remote", I64), ("local_chunks", I64),
-                ("remote_chunks", I64), ("remote_cols", I64), ("device_bytes", I64)]
+                ("remote_chunks", I64), ("remote_cols", I64), ("device_bytes", I64), ("hub_rows", I64),
+                ("hub_segments", I64), ("row_tasks", I64)]
 
 
 class ZipView(ctypes.Structure):
@@ -59,7 +62,8 @@ class ZipView(ctypes.Structure):
 
 
 class SpmmOpts(ctypes.Structure):
-    _fields_ = [("accumulate", I32), ("schedule", I32), ("gather_batch_rows", I32), ("reserved", I32 * 5)]
+    _fields_ = [("accumulate", I32), ("schedule", I32), ("gather_batch_rows", I32), ("unroll", I32),
+                ("min_blocks", I32), ("reserved", I32 * 3)]
 
 
 # name -> (restype, argtypes)

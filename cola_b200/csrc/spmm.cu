@@ -14,6 +14,7 @@
 #include "common.h"
 #include "prep.h"
 #include "spmm_kernels.cuh"
+#include "spmm_rows.cuh"
 
 using cola::dev::GatherSeg;
 using cola::dev::PartDesc;
@@ -190,6 +191,150 @@ static cola_status launch_gather(const GatherSeg *segs, const GatherSeg &single,
 #undef COLA_GATHER
     COLA_CUDA(cudaGetLastError());
     return COLA_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// row-major schedule dispatch
+// ---------------------------------------------------------------------------
+struct RowsLaunch {
+    dev::RowsArgs ra;
+    const void *X;
+    int64_t ldx;
+    void *Y;
+    int64_t ldy;
+    int K;
+    cola_dtype xdt, ydt;
+    bool vec;
+    int accumulate;
+    int unroll;
+    int min_blocks;
+};
+
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC>
+static cola_status launch_rows_t(const RowsLaunch &a, cudaStream_t st)
+{
+    using T = typename dev::ElemOf<TR>::T;
+    constexpr int W = LG * NV * TR::E;
+    auto fn = dev::rows_spmm_kernel<TR, TY, LG, NV, UNROLL, VEC>;
+    const int64_t gx = grid_for((const void *)fn, a.ra.nseg + a.ra.nrows);
+    const int gy = (a.K + W - 1) / W;
+    fn<<<dim3((unsigned)gx, (unsigned)gy), dev::kThreads, 0, st>>>(a.ra, static_cast<const T *>(a.X), a.ldx,
+                                                                   static_cast<TY *>(a.Y), a.ldy, a.K, a.accumulate);
+    COLA_CUDA(cudaGetLastError());
+    return COLA_SUCCESS;
+}
+
+template <typename TR, typename TY, bool VEC>
+static cola_status launch_rows_geo(const RowsLaunch &a, int V, cudaStream_t st)
+{
+    if (V <= 1)
+        return launch_rows_t<TR, TY, 1, 1, 4, VEC>(a, st);
+    if (V <= 2)
+        return launch_rows_t<TR, TY, 2, 1, 4, VEC>(a, st);
+    if (V <= 4)
+        return launch_rows_t<TR, TY, 4, 1, 4, VEC>(a, st);
+    if (V <= 8)
+        return launch_rows_t<TR, TY, 8, 1, 4, VEC>(a, st);
+    if (V <= 16)
+        return launch_rows_t<TR, TY, 16, 1, 4, VEC>(a, st);
+    if (V <= 32) {
+        if (a.unroll == 8)
+            return launch_rows_t<TR, TY, 32, 1, 8, VEC>(a, st);
+        if (a.unroll == 2)
+            return launch_rows_t<TR, TY, 32, 1, 2, VEC>(a, st);
+        return launch_rows_t<TR, TY, 32, 1, 4, VEC>(a, st);
+    }
+    if (V <= 64) {
+        if (a.unroll == 4 || a.unroll == 8)
+            return launch_rows_t<TR, TY, 32, 2, 4, VEC>(a, st);
+        return launch_rows_t<TR, TY, 32, 2, 2, VEC>(a, st);
+    }
+    return launch_rows_t<TR, TY, 32, 4, 2, VEC>(a, st);
+}
+
+static cola_status launch_rows(const RowsLaunch &a, cudaStream_t st)
+{
+    if (a.ra.nseg + a.ra.nrows <= 0 || a.K <= 0)
+        return COLA_SUCCESS;
+    using BF = __nv_bfloat16;
+    if (a.xdt == COLA_FLOAT32) {
+        if (a.ydt == COLA_FLOAT32)
+            return a.vec ? launch_rows_geo<dev::VecTraits<float>, float, true>(a, a.K / 4, st)
+                         : launch_rows_geo<dev::ScalarTraits<float>, float, false>(a, a.K, st);
+        return a.vec ? launch_rows_geo<dev::VecTraits<float>, BF, true>(a, a.K / 4, st)
+                     : launch_rows_geo<dev::ScalarTraits<float>, BF, false>(a, a.K, st);
+    }
+    if (a.ydt == COLA_FLOAT32)
+        return a.vec ? launch_rows_geo<dev::VecTraits<BF>, float, true>(a, a.K / 8, st)
+                     : launch_rows_geo<dev::ScalarTraits<BF>, float, false>(a, a.K, st);
+    return a.vec ? launch_rows_geo<dev::VecTraits<BF>, BF, true>(a, a.K / 8, st)
+                 : launch_rows_geo<dev::ScalarTraits<BF>, BF, false>(a, a.K, st);
+}
+
+template <typename TR, typename TY, int NV, int UNROLL, bool VEC, int MINB = 1>
+static cola_status launch_block_t(const dev::BlockArgs &ba, const RowsLaunch &a, cudaStream_t st)
+{
+    using T = typename dev::ElemOf<TR>::T;
+    constexpr int W = 32 * NV * TR::E;
+    auto fn = dev::rowblock_spmm_kernel<TR, TY, NV, UNROLL, VEC, MINB>;
+    const int64_t gx = grid_for((const void *)fn, ba.nseg + ba.ntask);
+    const int gy = (a.K + W - 1) / W;
+    fn<<<dim3((unsigned)gx, (unsigned)gy), dev::kThreads, 0, st>>>(ba, static_cast<const T *>(a.X), a.ldx,
+                                                                   static_cast<TY *>(a.Y), a.ldy, a.K, a.accumulate);
+    COLA_CUDA(cudaGetLastError());
+    return COLA_SUCCESS;
+}
+
+template <typename TR, typename TY>
+static cola_status launch_block_geo(const dev::BlockArgs &ba, const RowsLaunch &a, int V, cudaStream_t st)
+{
+    if (V <= 32) {
+        if (a.unroll == 8)
+            return launch_block_t<TR, TY, 1, 8, true>(ba, a, st);
+        if (a.unroll == 2)
+            return launch_block_t<TR, TY, 1, 2, true>(ba, a, st);
+        if (a.unroll == 6)
+            return launch_block_t<TR, TY, 1, 6, true>(ba, a, st);
+        if (a.min_blocks == 3)
+            return launch_block_t<TR, TY, 1, 4, true, 3>(ba, a, st);
+        if (a.min_blocks == 5)
+            return launch_block_t<TR, TY, 1, 4, true, 5>(ba, a, st);
+        if (a.min_blocks == 6)
+            return launch_block_t<TR, TY, 1, 4, true, 6>(ba, a, st);
+        return launch_block_t<TR, TY, 1, 4, true, 4>(ba, a, st);
+    }
+    if (V <= 64) {
+        if (a.unroll == 4 || a.unroll == 8)
+            return launch_block_t<TR, TY, 2, 4, true>(ba, a, st);
+        return launch_block_t<TR, TY, 2, 2, true>(ba, a, st);
+    }
+    return launch_block_t<TR, TY, 4, 2, true>(ba, a, st);
+}
+
+// Row-block streaming launch for rows one warp wide (vector path, V > 16).
+static cola_status launch_block(const dev::BlockArgs &ba, const RowsLaunch &a, cudaStream_t st)
+{
+    if (ba.nseg + ba.ntask <= 0)
+        return COLA_SUCCESS;
+    using BF = __nv_bfloat16;
+    if (a.xdt == COLA_FLOAT32)
+        return a.ydt == COLA_FLOAT32 ? launch_block_geo<dev::VecTraits<float>, float>(ba, a, a.K / 4, st)
+                                     : launch_block_geo<dev::VecTraits<float>, BF>(ba, a, a.K / 4, st);
+    return a.ydt == COLA_FLOAT32 ? launch_block_geo<dev::VecTraits<BF>, float>(ba, a, a.K / 8, st)
+                                 : launch_block_geo<dev::VecTraits<BF>, BF>(ba, a, a.K / 8, st);
+}
+
+// Vector path of the row-major schedule: X rows in 16-byte vectors, Y rows
+// written E elements at a time (E*sizeof(TY) bytes, aligned).
+static bool vec_ok_rows(cola_dtype xdt, const void *X, int64_t ldx, cola_dtype ydt, const void *Y, int64_t ldy, int K)
+{
+    const int E = xdt == COLA_FLOAT32 ? 4 : 8;
+    const int ysz = ydt == COLA_FLOAT32 ? 4 : 2;
+    if (K % E || ldx % E || !aligned16(X))
+        return false;
+    if (ldy % E || ((uintptr_t)Y % (uintptr_t)(E * ysz)) != 0)
+        return false;
+    return true;
 }
 
 static PartDesc part_desc_zero()
@@ -407,6 +552,20 @@ struct cola_graph {
     size_t ws_bytes = 0;
     GatherSeg *d_bufsegs = nullptr;  // BUFFER schedule gather segments
     std::vector<GatherSeg> h_bufsegs;
+    // row-major view (ROWS schedule): merged local + transposed remote entries
+    bool has_rows = false;
+    const int64_t *rv_ptr = nullptr;  // N+1
+    const int32_t *rv_col = nullptr;
+    const float *rv_val = nullptr;
+    const int32_t *seg_row = nullptr;
+    const int64_t *seg_beg = nullptr;
+    const int32_t *hub_row = nullptr;
+    const int64_t *hub_seg = nullptr;
+    const int32_t *task_rb = nullptr, *task_re = nullptr;
+    int64_t nseg = 0, nhub = 0, ntask = 0;
+    int32_t hub_threshold = 256, hub_segment = 256, task_entries = 256;
+    float *ws_hub = nullptr;  // nseg x K partials
+    size_t ws_hub_bytes = 0;
 };
 
 namespace cola {
@@ -435,6 +594,7 @@ static void graph_release(cola_graph *g)
     cudaFree(g->ppl_buf);
     cudaFree(g->stage_buf);
     cudaFree(g->ws);
+    cudaFree(g->ws_hub);
     cudaSetDevice(cur);
     delete g;
 }
@@ -516,6 +676,103 @@ static cola_status graph_upload(const cola_partition_set *ps, const cola_upload_
                                   g->tables[(size_t)p]));
     }
 
+    // row-major view: per output row, its remote entries left of the
+    // partition's own columns, its local entries, then the remote entries to
+    // the right -- i.e. ascending global column order
+    const bool rows = !(opts && opts->no_row_view);
+    std::vector<int64_t> rv_ptr;
+    std::vector<int32_t> rv_col, seg_row, hub_row;
+    std::vector<float> rv_val;
+    std::vector<int64_t> seg_beg, hub_seg;
+    std::vector<int32_t> task_rb, task_re;
+    if (rows) {
+        const int64_t N = g->N;
+        g->hub_threshold = opts && opts->hub_threshold > 0 ? opts->hub_threshold : 256;
+        g->hub_segment = opts && opts->hub_segment > 0 ? opts->hub_segment : 256;
+        rv_ptr.assign((size_t)N + 1, 0);
+        for (const PartHost &ph : ps->parts) {
+            for (size_t i = 0; i < ph.l_rowIdx.size(); i++)
+                rv_ptr[(size_t)(ph.row_lb + ph.l_rowIdx[i]) + 1] += ph.l_rowPtr[i + 1] - ph.l_rowPtr[i];
+            for (int32_t r : ph.r_rowIdx)
+                rv_ptr[(size_t)(ph.row_lb + r) + 1] += 1;
+        }
+        for (int64_t r = 0; r < N; r++)
+            rv_ptr[(size_t)r + 1] += rv_ptr[(size_t)r];
+        rv_col.resize((size_t)rv_ptr[(size_t)N]);
+        rv_val.resize((size_t)rv_ptr[(size_t)N]);
+        std::vector<int64_t> cur(rv_ptr.begin(), rv_ptr.end() - 1);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int32_t p = 0; p < P; p++) {
+            const PartHost &ph = ps->parts[(size_t)p];
+            const int64_t clb = (int64_t)p * ps->npp;
+            size_t ci = 0;
+            auto remote_cols_below = [&](int64_t limit) {
+                for (; ci < ph.r_colIdx.size() && ph.r_colIdx[ci] < limit; ci++)
+                    for (int32_t q = ph.r_colPtr[ci]; q < ph.r_colPtr[ci + 1]; q++) {
+                        const int64_t row = ph.row_lb + ph.r_rowIdx[(size_t)q];
+                        const int64_t at = cur[(size_t)row]++;
+                        rv_col[(size_t)at] = ph.r_colIdx[ci];
+                        rv_val[(size_t)at] = ph.r_val[(size_t)q];
+                    }
+            };
+            remote_cols_below(clb);
+            for (size_t i = 0; i < ph.l_rowIdx.size(); i++) {
+                const int64_t row = ph.row_lb + ph.l_rowIdx[i];
+                for (int32_t q = ph.l_rowPtr[i]; q < ph.l_rowPtr[i + 1]; q++) {
+                    const int64_t at = cur[(size_t)row]++;
+                    rv_col[(size_t)at] = (int32_t)(clb + ph.l_colIdx[(size_t)q]);
+                    rv_val[(size_t)at] = ph.l_val[(size_t)q];
+                }
+            }
+            remote_cols_below(INT64_MAX);
+        }
+        // hub rows -> fixed-length segments
+        for (int64_t r = 0; r < N; r++) {
+            const int64_t b = rv_ptr[(size_t)r], e = rv_ptr[(size_t)r + 1];
+            if (e - b <= g->hub_threshold)
+                continue;
+            hub_row.push_back((int32_t)r);
+            hub_seg.push_back((int64_t)seg_row.size());
+            for (int64_t q = b; q < e; q += g->hub_segment) {
+                seg_row.push_back((int32_t)r);
+                seg_beg.push_back(q);
+            }
+        }
+        hub_seg.push_back((int64_t)seg_row.size());
+        g->nseg = (int64_t)seg_row.size();
+        g->nhub = (int64_t)hub_row.size();
+        // row blocks of about task_entries entries (a row costs its entries
+        // plus 2 for its write), never containing a hub row
+        g->task_entries = opts && opts->task_entries > 0 ? opts->task_entries : 128;
+        int64_t start = -1, cost = 0;
+        for (int64_t r = 0; r < N; r++) {
+            const int64_t len = rv_ptr[(size_t)r + 1] - rv_ptr[(size_t)r];
+            if (len > g->hub_threshold) {
+                if (start >= 0) {
+                    task_rb.push_back((int32_t)start);
+                    task_re.push_back((int32_t)r);
+                }
+                start = -1;
+                cost = 0;
+                continue;
+            }
+            if (start < 0)
+                start = r;
+            cost += len + 2;
+            if (cost >= g->task_entries) {
+                task_rb.push_back((int32_t)start);
+                task_re.push_back((int32_t)(r + 1));
+                start = -1;
+                cost = 0;
+            }
+        }
+        if (start >= 0) {
+            task_rb.push_back((int32_t)start);
+            task_re.push_back((int32_t)N);
+        }
+        g->ntask = (int64_t)task_rb.size();
+    }
+
     // one device allocation for everything
     Arena ar;
     struct Offs {
@@ -561,11 +818,36 @@ static cola_status graph_upload(const cola_partition_set *ps, const cola_upload_
         }
     }
     const size_t desc_buf = ar.add(nullptr, (size_t)P * sizeof(GatherSeg));
+    size_t o_rv_ptr = 0, o_rv_col = 0, o_rv_val = 0, o_seg_row = 0, o_seg_beg = 0, o_hub_row = 0, o_hub_seg = 0;
+    size_t o_task_rb = 0, o_task_re = 0;
+    if (rows) {
+        o_rv_ptr = ar.add(rv_ptr.data(), rv_ptr.size() * 8);
+        o_rv_col = ar.add(rv_col.data(), rv_col.size() * 4);
+        o_rv_val = ar.add(rv_val.data(), rv_val.size() * 4);
+        o_seg_row = ar.add(seg_row.data(), seg_row.size() * 4);
+        o_seg_beg = ar.add(seg_beg.data(), seg_beg.size() * 8);
+        o_hub_row = ar.add(hub_row.data(), hub_row.size() * 4);
+        o_hub_seg = ar.add(hub_seg.data(), hub_seg.size() * 8);
+        o_task_rb = ar.add(task_rb.data(), task_rb.size() * 4);
+        o_task_re = ar.add(task_re.data(), task_re.size() * 4);
+    }
     ar.total = std::max<size_t>(ar.total, 256);
     COLA_CUDA(cudaMalloc(&g->dmem, ar.total));
     g->dbytes = ar.total;
     char *base = static_cast<char *>(g->dmem);
     auto at = [&](size_t o) { return reinterpret_cast<const int32_t *>(base + o); };
+    if (rows) {
+        g->has_rows = true;
+        g->rv_ptr = reinterpret_cast<const int64_t *>(base + o_rv_ptr);
+        g->rv_col = at(o_rv_col);
+        g->rv_val = reinterpret_cast<const float *>(base + o_rv_val);
+        g->seg_row = at(o_seg_row);
+        g->seg_beg = reinterpret_cast<const int64_t *>(base + o_seg_beg);
+        g->hub_row = at(o_hub_row);
+        g->hub_seg = reinterpret_cast<const int64_t *>(base + o_hub_seg);
+        g->task_rb = at(o_task_rb);
+        g->task_re = at(o_task_re);
+    }
 
     // descriptors
     g->zips.resize((size_t)P);
@@ -728,7 +1010,10 @@ cola_status cola_graph_get_info(const cola_graph *g, cola_graph_info *o)
     o->local_chunks = g->lchunks;
     o->remote_chunks = g->rchunks;
     o->remote_cols = g->rcols;
-    o->device_bytes = (int64_t)(g->dbytes + g->ppl_bytes + g->stage_bytes + g->ws_bytes);
+    o->device_bytes = (int64_t)(g->dbytes + g->ppl_bytes + g->stage_bytes + g->ws_bytes + g->ws_hub_bytes);
+    o->hub_rows = g->nhub;
+    o->hub_segments = g->nseg;
+    o->row_tasks = g->ntask;
     return COLA_SUCCESS;
 }
 
@@ -755,7 +1040,11 @@ cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype xdt, int64_t ldx,
     COLA_REQUIRE(!(accumulate && ydt != COLA_FLOAT32), COLA_ERROR_UNSUPPORTED,
                  "cola_spmm: accumulate needs an FP32 Y");
     if (schedule == COLA_SCHEDULE_AUTO)
-        schedule = g->nstages > 1 ? COLA_SCHEDULE_PIPELINE : COLA_SCHEDULE_FUSED;
+        schedule = g->has_rows ? COLA_SCHEDULE_ROWS : (g->nstages > 1 ? COLA_SCHEDULE_PIPELINE : COLA_SCHEDULE_FUSED);
+    COLA_REQUIRE(schedule != COLA_SCHEDULE_ROWS || g->has_rows, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_spmm: the row-major schedule needs a graph uploaded with its row view");
+    COLA_REQUIRE(schedule >= COLA_SCHEDULE_FUSED && schedule <= COLA_SCHEDULE_ROWS, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_spmm: unknown schedule %d", schedule);
     COLA_REQUIRE(schedule != COLA_SCHEDULE_PIPELINE || g->nstages > 1, COLA_ERROR_INVALID_ARGUMENT,
                  "cola_spmm: the pipelined schedule needs a graph uploaded with group_size < nparts");
     int cur = 0;
@@ -765,6 +1054,66 @@ cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype xdt, int64_t ldx,
     cudaStream_t st = (cudaStream_t)stream;
     if (g->N == 0)
         return COLA_SUCCESS;
+
+    if (schedule == COLA_SCHEDULE_ROWS) {
+        // one writer per output row: Y written directly in its own dtype
+        if (g->nseg > 0)
+            COLA_TRY(ensure(reinterpret_cast<void *&>(g->ws_hub), g->ws_hub_bytes, (size_t)g->nseg * K * sizeof(float)));
+        RowsLaunch a;
+        a.ra.rowptr = g->rv_ptr;
+        a.ra.col = g->rv_col;
+        a.ra.val = g->rv_val;
+        a.ra.nrows = g->N;
+        a.ra.hub_threshold = g->hub_threshold;
+        a.ra.seg_row = g->seg_row;
+        a.ra.seg_beg = g->seg_beg;
+        a.ra.nseg = g->nseg;
+        a.ra.seg_len = g->hub_segment;
+        a.ra.ws = g->ws_hub;
+        a.ra.ld_ws = K;
+        a.X = X;
+        a.ldx = ldx;
+        a.Y = Y;
+        a.ldy = ldy;
+        a.K = K;
+        a.xdt = xdt;
+        a.ydt = ydt;
+        a.vec = vec_ok_rows(xdt, X, ldx, ydt, Y, ldy, K);
+        a.accumulate = accumulate;
+        a.unroll = opts ? opts->unroll : 0;
+        a.min_blocks = opts ? opts->min_blocks : 0;
+        const int V = a.vec ? K / (xdt == COLA_FLOAT32 ? 4 : 8) : 0;
+        if (a.vec && V > 16) {
+            dev::BlockArgs ba;
+            ba.rowptr = g->rv_ptr;
+            ba.col = g->rv_col;
+            ba.val = g->rv_val;
+            ba.task_rb = g->task_rb;
+            ba.task_re = g->task_re;
+            ba.ntask = g->ntask;
+            ba.seg_row = g->seg_row;
+            ba.seg_beg = g->seg_beg;
+            ba.nseg = g->nseg;
+            ba.seg_len = g->hub_segment;
+            ba.ws = g->ws_hub;
+            ba.ld_ws = K;
+            COLA_TRY(launch_block(ba, a, st));
+        } else {
+            COLA_TRY(launch_rows(a, st));
+        }
+        if (g->nhub > 0) {
+            const int64_t blocks = (g->nhub + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock;
+            if (ydt == COLA_FLOAT32)
+                dev::hub_combine_kernel<float><<<(unsigned)blocks, dev::kThreads, 0, st>>>(
+                    g->hub_row, g->hub_seg, g->nhub, g->ws_hub, K, static_cast<float *>(Y), ldy, K, accumulate);
+            else
+                dev::hub_combine_kernel<__nv_bfloat16><<<(unsigned)blocks, dev::kThreads, 0, st>>>(
+                    g->hub_row, g->hub_seg, g->nhub, g->ws_hub, K, static_cast<__nv_bfloat16 *>(Y), ldy, K,
+                    accumulate);
+            COLA_CUDA(cudaGetLastError());
+        }
+        return COLA_SUCCESS;
+    }
 
     // accumulation target
     float *acc = nullptr;

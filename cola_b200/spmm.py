@@ -11,7 +11,7 @@ import torch
 
 from . import _lib
 from ._lib import (BFLOAT16, FLOAT32, SCHEDULE_AUTO, SCHEDULE_BUFFER, SCHEDULE_FUSED,  # noqa: F401
-                   SCHEDULE_PIPELINE, GraphInfo, SpmmOpts, UploadOpts, ZipView, check, lib)
+                   SCHEDULE_PIPELINE, SCHEDULE_ROWS, GraphInfo, SpmmOpts, UploadOpts, ZipView, check, lib)
 
 _DT = {torch.float32: FLOAT32, torch.bfloat16: BFLOAT16}
 
@@ -43,10 +43,15 @@ class Graph:
     (the d_csr_zip / d_csc_zip holders of include/sparse_data.h for every PE,
     plus the pipelined schedule's stage tables)."""
 
-    def __init__(self, pset, if_split=True, group_size=None, stream=None):
+    def __init__(self, pset, if_split=True, group_size=None, row_view=True, hub_threshold=0, hub_segment=0,
+                 task_entries=0, stream=None):
         o = UploadOpts()
         o.if_split = 1 if if_split else 0
         o.group_size = int(group_size or 0)
+        o.no_row_view = 0 if row_view else 1
+        o.hub_threshold = int(hub_threshold)
+        o.hub_segment = int(hub_segment)
+        o.task_entries = int(task_entries)
         h = ctypes.c_void_p()
         check(lib().cola_graph_upload(pset.handle, ctypes.byref(o), ctypes.byref(h), _stream(stream)))
         self._h = h
@@ -66,7 +71,7 @@ class Graph:
         return z
 
     def spmm(self, X, Y=None, out_dtype=None, accumulate=False, schedule=SCHEDULE_AUTO, gather_batch_rows=0,
-             stream=None):
+             unroll=0, min_blocks=0, stream=None):
         """Y = A X (Y += A X with accumulate).  X: (>= N) x K CUDA tensor,
         float32 or bfloat16; Y: N x K float32 or bfloat16 (allocated when None)."""
         _dense(X, "X")
@@ -82,6 +87,8 @@ class Graph:
         o.accumulate = 1 if accumulate else 0
         o.schedule = int(schedule)
         o.gather_batch_rows = int(gather_batch_rows)
+        o.unroll = int(unroll)
+        o.min_blocks = int(min_blocks)
         check(lib().cola_spmm(self._h, _ptr(X), _DT[X.dtype], X.stride(0), _ptr(Y), _DT[Y.dtype], Y.stride(0), K,
                               ctypes.byref(o), _stream(stream)))
         return Y

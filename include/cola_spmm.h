@@ -221,9 +221,13 @@ cola_status cola_batching_data_ppl(const float *input, float *send, const int32_
 typedef struct cola_graph cola_graph;
 
 typedef struct cola_upload_opts {
-    int32_t if_split;    /* nnz_split the remote CSC too (src/distSpMM_ppl_batch.cu:86-98); 1 = yes */
-    int32_t group_size;  /* work-group size for the pipelined schedule; 0 or nparts = single stage */
-    int32_t reserved[6];
+    int32_t if_split;       /* nnz_split the remote CSC too (src/distSpMM_ppl_batch.cu:86-98); 1 = yes */
+    int32_t group_size;     /* work-group size for the pipelined schedule; 0 or nparts = single stage */
+    int32_t no_row_view;    /* 1: skip the row-major view (COLA_SCHEDULE_ROWS unavailable, less memory) */
+    int32_t hub_threshold;  /* ROWS: rows with more entries are split into segments; 0 = 256 */
+    int32_t hub_segment;    /* ROWS: entries per hub segment; 0 = 256 */
+    int32_t task_entries;   /* ROWS: entries per row-block task (one warp each); 0 = 128 */
+    int32_t reserved[2];
 } cola_upload_opts;
 
 /* Splits, builds stage tables and uploads every partition to the current
@@ -237,6 +241,8 @@ typedef struct cola_graph_info {
     int64_t nnz, nnz_local, nnz_remote;
     int64_t local_chunks, remote_chunks, remote_cols;
     int64_t device_bytes;
+    int64_t hub_rows, hub_segments;  /* ROWS schedule */
+    int64_t row_tasks;               /* ROWS schedule: row blocks of about task_entries entries */
 } cola_graph_info;
 cola_status cola_graph_get_info(const cola_graph *g, cola_graph_info *out);
 
@@ -256,14 +262,19 @@ enum cola_schedule {
     COLA_SCHEDULE_AUTO = 0,     /* pick by measurement / tuning cache */
     COLA_SCHEDULE_FUSED = 1,    /* one launch: local CSR + remote CSC, rows staged on chip */
     COLA_SCHEDULE_BUFFER = 2,   /* remote rows gathered into an HBM staging buffer in batches first */
-    COLA_SCHEDULE_PIPELINE = 3  /* the reference's multi-stage work-group schedule */
+    COLA_SCHEDULE_PIPELINE = 3, /* the reference's multi-stage work-group schedule */
+    COLA_SCHEDULE_ROWS = 4      /* row-major view (remote CSC transposed at upload, merged with the
+                                   local CSR): one writer per output row, no atomics, deterministic;
+                                   hub rows split into segments combined pairwise */
 };
 
 typedef struct cola_spmm_opts {
     int32_t accumulate;         /* 0: Y is overwritten; 1: Y += A X (Y must be FP32) */
     int32_t schedule;           /* enum cola_schedule */
     int32_t gather_batch_rows;  /* staging batch (rows) for BUFFER/PIPELINE; 0 = 4096 */
-    int32_t reserved[5];
+    int32_t unroll;             /* ROWS: row loads in flight per lane group (2, 4, 6 or 8; 0 = 4) */
+    int32_t min_blocks;         /* ROWS: resident blocks per SM the kernel is compiled for (3, 5, 6; 0 = 4) */
+    int32_t reserved[3];
 } cola_spmm_opts;
 
 /* Y = A X (or Y += A X) for all partitions.  X: >= P*npp rows (rows past N are

@@ -339,3 +339,81 @@ def test_batching_data_ppl_matches_reference_bit_exact():
     cb._lib.check(cb.lib().cola_batching_data_ppl(ptr(X), ptr(b), ptr(idx), 700, K, npp, 1, None))
     torch.cuda.synchronize()
     assert torch.equal(a, b)
+
+
+# ---------------------------------------------------------------------------
+# row-major schedule (remote CSC transposed at upload; one writer per row)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("K", [1, 3, 16, 32, 33, 64, 96, 100, 128, 256, 512])
+def test_rows_fp32_matches_fp64(case12, K):
+    n, row, col, val, ps = case12
+    g = S.Graph(ps)
+    assert g.info.hub_rows > 0  # the R-MAT hubs exceed the default threshold
+    X = dense_x(n, K, seed=100 + K)
+    ref = fp64_reference(n, row, col, val, X)
+    Y = g.spmm(torch.from_numpy(X).to(DEV), schedule=S.SCHEDULE_ROWS)
+    torch.cuda.synchronize()
+    assert rel(Y.cpu().numpy(), ref) <= TOL_F32
+
+
+@pytest.mark.parametrize("thr,seg", [(0, 0), (8, 4), (1, 1), (40, 16), (10 ** 6, 256)])
+def test_rows_hub_segments(case12, thr, seg):
+    n, row, col, val, ps = case12
+    g = S.Graph(ps, hub_threshold=thr, hub_segment=seg)
+    X = dense_x(n, 64, seed=7)
+    ref = fp64_reference(n, row, col, val, X)
+    Y = g.spmm(torch.from_numpy(X).to(DEV), schedule=S.SCHEDULE_ROWS)
+    Y2 = g.spmm(torch.from_numpy(X).to(DEV), schedule=S.SCHEDULE_ROWS)
+    torch.cuda.synchronize()
+    assert rel(Y.cpu().numpy(), ref) <= TOL_F32
+    assert torch.equal(Y, Y2)  # no atomics: bitwise reproducible
+
+
+@pytest.mark.parametrize("K", [32, 64, 256])
+def test_rows_bf16_in_out(case12, K):
+    n, row, col, val, ps = case12
+    g = S.Graph(ps, hub_threshold=64, hub_segment=32)
+    X = dense_x(n, K, seed=9)
+    Xb = bf16_bits(X)
+    rp, ci, vv = oracle.global_csr(n, row, col, val)
+    ref_b = oracle.spmm_csr_f64(rp, ci, vv, Xb)
+    ref_f = oracle.spmm_csr_f64(rp, ci, vv, X)
+    xt = torch.from_numpy(Xb.view(np.int16)).view(torch.bfloat16).to(DEV)
+    xf = torch.from_numpy(X).to(DEV)
+    y32 = g.spmm(xt, out_dtype=torch.float32, schedule=S.SCHEDULE_ROWS)
+    y16 = g.spmm(xt, out_dtype=torch.bfloat16, schedule=S.SCHEDULE_ROWS)
+    yf16 = g.spmm(xf, out_dtype=torch.bfloat16, schedule=S.SCHEDULE_ROWS)
+    torch.cuda.synchronize()
+    assert rel(y32.cpu().numpy(), ref_b) <= TOL_F32
+    assert rel(y16.float().cpu().numpy(), ref_f) <= TOL_BF16
+    assert rel(yf16.float().cpu().numpy(), ref_f) <= TOL_BF16
+    # the BF16 output is the FP32 accumulation rounded once (same order: exact)
+    assert torch.equal(y16, y32.to(torch.bfloat16))
+
+
+def test_rows_accumulate_strides_and_agreement(case12):
+    n, row, col, val, ps = case12
+    g = S.Graph(ps, hub_threshold=32, hub_segment=16)
+    K = 64
+    X = dense_x(n, K, seed=12)
+    ref = fp64_reference(n, row, col, val, X)
+    big = torch.zeros((n, 80), device=DEV)
+    big[:, :K] = torch.from_numpy(X).to(DEV)
+    Y = torch.zeros((n, 72), device=DEV)
+    g.spmm(big[:, :K], Y[:, :K], schedule=S.SCHEDULE_ROWS)
+    g.spmm(big[:, :K], Y[:, :K], accumulate=True, schedule=S.SCHEDULE_ROWS)
+    yf = g.spmm(big[:, :K], schedule=S.SCHEDULE_FUSED)
+    torch.cuda.synchronize()
+    assert rel(Y[:, :K].cpu().numpy(), 2 * ref) <= TOL_F32
+    assert torch.all(Y[:, K:] == 0)
+    assert rel(yf.cpu().numpy(), Y[:, :K].cpu().numpy() / 2) <= TOL_F32
+
+
+def test_rows_view_optional(case12):
+    n, row, col, val, ps = case12
+    g = S.Graph(ps, row_view=False)
+    with pytest.raises(cb.ColaError):
+        g.spmm(torch.ones((n, 16), device=DEV), schedule=S.SCHEDULE_ROWS)
+    Y = g.spmm(torch.ones((n, 16), device=DEV))  # AUTO falls back to the fused schedule
+    torch.cuda.synchronize()
+    assert Y.shape == (n, 16)
