@@ -27,6 +27,9 @@ SCHEDULE_BUFFER = 2
 SCHEDULE_PIPELINE = 3
 SCHEDULE_ROWS = 4
 
+# capacity (floats) of the library's fixed staging array (include/cola_spmm.h)
+NOALLOC_STAGE_FLOATS = 2 * 1024 * 1024
+
 
 class ColaError(RuntimeError):
     def __init__(self, status, msg):
@@ -88,6 +91,7 @@ SIGNATURES = {
     "cola_ppl0_batch_spmm": (I32, [P, P] + [P] * 8 + [I32] * 7 + [P]),
     "cola_ppl0_batch_spmm_seq": (I32, [P, P] + [P] * 8 + [I32] * 7 + [P]),
     "cola_ppl0_batch_buffer_spmm": (I32, [P, P, P] + [P] * 8 + [I32] * 7 + [P]),
+    "cola_ppl0_batch_buffer_spmm_noalloc": (I32, [P, P] + [P] * 8 + [I32] * 7 + [P]),
     "cola_ppl_batch_spmm": (I32, [P, P, P, P, P, P] + [I32] * 5 + [P] + [I32] * 5 + [P]),
     "cola_batching_data_ppl": (I32, [P, P, P, I32, I32, I32, I32, P]),
     "cola_graph_upload": (I32, [P, P, P, P]),

@@ -1237,3 +1237,87 @@ cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype xdt, int64_t ldx,
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Buffer-staged launcher that allocates nothing: the remote rows are staged in
+// a fixed array compiled into the library instead of a caller buffer.
+// ===========================================================================
+static __device__ __align__(256) float g_noalloc_stage[COLA_NOALLOC_STAGE_FLOATS];
+
+namespace cola {
+
+// Device address of g_noalloc_stage on the current device.  In host code the
+// array's name only stands in for the symbol, so the address is looked up with
+// cudaGetSymbolAddress, once per device (the first call on each device).
+static cola_status noalloc_stage(float **out)
+{
+    static std::mutex mu;
+    static float *addr[64] = {nullptr};
+    int dev = 0;
+    COLA_CUDA(cudaGetDevice(&dev));
+    COLA_REQUIRE(dev >= 0 && dev < 64, COLA_ERROR_UNSUPPORTED, "noalloc staging: device %d out of range", dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        COLA_CUDA(cudaGetSymbolAddress(&p, g_noalloc_stage));
+        addr[dev] = static_cast<float *>(p);
+    }
+    *out = addr[dev];
+    return COLA_SUCCESS;
+}
+
+}  // namespace cola
+
+extern "C" cola_status cola_ppl0_batch_buffer_spmm_noalloc(
+    float *output, const float *input, const int32_t *csr_rowPtr_l, const int32_t *csr_colIdx_l,
+    const int32_t *csr_rowIdx_zip_l, const float *csr_val_l, const int32_t *csc_colPtr_r, const int32_t *csc_rowIdx_r,
+    const int32_t *csc_colIdx_zip_r, const float *csc_val_r, int32_t local_row_lb, int32_t remote_col_lb,
+    int32_t local_row_num, int32_t remote_col_num, int32_t dim, int32_t nodesPerPE, int32_t peid,
+    cola_stream_t stream)
+{
+    (void)local_row_lb;
+    COLA_TRY(check_dim(dim, nodesPerPE));
+    COLA_REQUIRE(local_row_num >= 0 && remote_col_num >= 0 && remote_col_lb >= 0 && peid >= 0,
+                 COLA_ERROR_INVALID_ARGUMENT, "cola_ppl0_batch_buffer_spmm_noalloc: negative count or offset");
+    const int64_t need = (int64_t)remote_col_num * dim;
+    COLA_REQUIRE(need <= (int64_t)COLA_NOALLOC_STAGE_FLOATS, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_ppl0_batch_buffer_spmm_noalloc: %d remote rows x dim %d need %lld staging floats, the "
+                 "library's fixed array holds %u (use cola_ppl0_batch_buffer_spmm with a caller buffer)",
+                 remote_col_num, dim, (long long)need, (unsigned)COLA_NOALLOC_STAGE_FLOATS);
+    const int64_t T = (int64_t)local_row_num + remote_col_num;
+    if (T == 0)
+        return COLA_SUCCESS;
+    COLA_REQUIRE(output && input, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_ppl0_batch_buffer_spmm_noalloc: null dense pointer");
+    float *stage = nullptr;
+    COLA_TRY(noalloc_stage(&stage));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (remote_col_num > 0) {
+        // every staged row read below is written here first
+        GatherSeg s;
+        std::memset(&s, 0, sizeof s);
+        s.idx = csc_colIdx_zip_r + remote_col_lb;
+        s.n = remote_col_num;
+        s.src_row0 = -(int64_t)peid * nodesPerPE;
+        s.dst_row0 = 0;
+        COLA_TRY(launch_gather(nullptr, s, 1, remote_col_num, input, dim, stage, dim, dim, COLA_FLOAT32, st));
+    }
+    PartDesc d = part_desc_zero();
+    d.l_ptr = csr_rowPtr_l;
+    d.l_col = csr_colIdx_l;
+    d.l_row = csr_rowIdx_zip_l;
+    d.l_val = csr_val_l;
+    d.r_ptr = csc_colPtr_r;
+    d.r_row = csc_rowIdx_r;
+    d.r_col = csc_colIdx_zip_r;
+    d.r_val = csc_val_r;
+    d.l_num = local_row_num;
+    d.r_begin = remote_col_lb;
+    d.r_num = remote_col_num;
+    d.r_mode = dev::kRemoteStagedChunk;
+    d.stage = stage;
+    d.ld_stage = dim;
+    FusedArgs a{nullptr, d, 1, T, input, dim, output, dim, dim, COLA_FLOAT32,
+                vec_ok(COLA_FLOAT32, input, dim, stage, dim, output, dim, dim)};
+    return launch_fused(a, st);
+}

@@ -195,6 +195,34 @@ cola_status cola_ppl0_batch_buffer_spmm(float *output, const float *input, float
                                         int32_t remote_col_num, int32_t dim, int32_t nodesPerPE, int32_t peid,
                                         cola_stream_t stream);
 
+/* Capacity, in floats, of the library's own staging array used by
+ * cola_ppl0_batch_buffer_spmm_noalloc (8 MiB; every GPU that loads the library
+ * holds it until the process exits). */
+#define COLA_NOALLOC_STAGE_FLOATS (2u * 1024u * 1024u)
+
+/* No counterpart in the reference.  The same computation as
+ * cola_ppl0_batch_buffer_spmm for callers that cannot allocate device memory
+ * and have none to lend: code running under a host framework that owns every
+ * device allocation, or a latency-bound loop that must not call cudaMalloc
+ * (it synchronises the device and can fail under memory pressure).  Instead of
+ * a caller-provided comm_buffer, the remote rows are staged in a fixed array
+ * inside the library, so this call allocates nothing.
+ * Limit: remote_col_num * dim must not exceed COLA_NOALLOC_STAGE_FLOATS;
+ * larger requests return COLA_ERROR_INVALID_ARGUMENT and launch nothing.
+ * The first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (on different streams, or from
+ * different threads) race on it and must be serialised by the caller.  The
+ * array keeps whatever the last call left in it; every call overwrites the
+ * rows it reads before reading them. */
+cola_status cola_ppl0_batch_buffer_spmm_noalloc(float *output, const float *input, const int32_t *csr_rowPtr_l,
+                                                const int32_t *csr_colIdx_l, const int32_t *csr_rowIdx_zip_l,
+                                                const float *csr_val_l, const int32_t *csc_colPtr_r,
+                                                const int32_t *csc_rowIdx_r, const int32_t *csc_colIdx_zip_r,
+                                                const float *csc_val_r, int32_t local_row_lb, int32_t remote_col_lb,
+                                                int32_t local_row_num, int32_t remote_col_num, int32_t dim,
+                                                int32_t nodesPerPE, int32_t peid, cola_stream_t stream);
+
 /* ppl_batch_SpMM (include/dist_spmm_ppl_batch.cuh:709-760): stage-i CSC
  * scatter over remote chunks [remote_col_lb, remote_col_ub).  Chunks in
  * [local_col_lb, local_col_ub) read row idx_ppl[w] of `input` (this PE's
