@@ -43,6 +43,9 @@ WORKLOADS = {
     "bf16": dict(scale=21, deg=48, K=256, P=8, xdt="bf16", ydt="bf16", seed=3,
                  desc="R-MAT scale 21 (2,097,152 nodes), avg degree 48, D^-1/2 A D^-1/2; X 2,097,152x256 BF16 "
                       "(from FP32 N(0,1)), FP32 accumulation, BF16 output; P=8 virtual row partitions"),
+    "fp32-k256": dict(scale=21, deg=48, K=256, P=8, xdt="fp32", ydt="fp32", seed=3,
+                      desc="R-MAT scale 21 (2,097,152 nodes), avg degree 48, D^-1/2 A D^-1/2; X 2,097,152x256 "
+                           "FP32; P=8 virtual row partitions (the plain FP32 path of the precision form)"),
 }
 METRIC = "SpMM HBM GB/s (algorithmic bytes / step time)"
 
@@ -119,6 +122,34 @@ def make_graph(w):
 def dense_x(n, K, seed):
     g = np.random.Generator(np.random.Philox(seed))
     return g.standard_normal((n, K), dtype=np.float32)
+
+
+def fp64_error(n, row, col, val, Xh, Y, dev, samples=4096):
+    """Relative Frobenius error of Y on a row sample (evenly spaced rows plus
+    the 16 longest rows) against Y = A X computed in FP64 on the GPU from the
+    FP32 features -- FP64 is used only in this validation reduction."""
+    import torch
+    counts = np.bincount(row, minlength=n)
+    rowptr = np.zeros(n + 1, np.int64)
+    np.cumsum(counts, out=rowptr[1:])
+    pick = np.unique(np.concatenate([np.linspace(0, n - 1, samples).astype(np.int64),
+                                     np.argsort(counts)[-16:].astype(np.int64)]))
+    crow = [0]
+    cols, vals = [], []
+    for r in pick:
+        a, b = rowptr[r], rowptr[r + 1]
+        cols.append(col[a:b])
+        vals.append(val[a:b])
+        crow.append(crow[-1] + (b - a))
+    A = torch.sparse_csr_tensor(torch.tensor(crow, dtype=torch.int64), torch.from_numpy(np.concatenate(cols).astype(np.int64)),
+                                torch.from_numpy(np.concatenate(vals).astype(np.float64)), size=(len(pick), n),
+                                device=dev)
+    X64 = torch.from_numpy(Xh).to(dev).double()
+    ref = (A @ X64)
+    got = Y[torch.from_numpy(pick).to(dev)].double()
+    err = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+    del X64
+    return err, int(len(pick))
 
 
 def read_traffic(name):
@@ -342,10 +373,12 @@ def run_ours(args, w):
         e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
         barrier()
 
+    err, nsamp = fp64_error(n, row, col, val, Xh, Y, dev)
     peak, peak_kind = measured_peak()
     achieved = B / (k_ms * 1e-3) / 1e9
-    traffic = read_traffic("fused_spmm_rmat20_k128_fp32.txt") if args.workload == "fp32" else \
-        read_traffic("fused_spmm_rmat21_k256_bf16.txt")
+    traffic = read_traffic({"fp32": "rowblock_spmm_rmat20_k128_fp32.md", "bf16": "rowblock_spmm_rmat21_k256_bf16.md",
+                            "fp32-k256": "rowblock_spmm_rmat21_k256_fp32.md"}[args.workload]) \
+        if eff == S.SCHEDULE_ROWS and args.scale is None else None
     if eff == S.SCHEDULE_ROWS:
         launches_per_step = 1 + (1 if info.hub_rows > 0 else 0)
     elif eff == S.SCHEDULE_FUSED:
@@ -374,6 +407,9 @@ def run_ours(args, w):
         "e2e": None if e2e_ms is None else {
             "value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": n * K * s_x,
             "d2h_bytes_per_step": n * K * s_y, "ms_per_step": e2e_ms},
+        "accuracy": {"rel_frobenius_vs_fp64": err, "rows_sampled": nsamp,
+                     "bound": 1e-5 if (xdt == torch.float32 and ydt == torch.float32) else 1e-2,
+                     "reference": "FP64 on the GPU from the FP32 features, sampled rows incl. the 16 longest"},
         "gpu_launches": (launches_per_step * args.steps) if launches_per_step else None,
         "clocks": clk,
     }
