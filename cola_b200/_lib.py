@@ -55,7 +55,7 @@ class GraphInfo(ctypes.Structure):
     _fields_ = [("num_nodes", I32), ("nparts", I32), ("nodes_per_part", I32), ("group_size", I32),
                 ("nnz", I64), ("nnz_local", I64), ("nnz_remote", I64), ("local_chunks", I64),
                 ("remote_chunks", I64), ("remote_cols", I64), ("device_bytes", I64), ("hub_rows", I64),
-                ("hub_segments", I64), ("row_tasks", I64)]
+                ("hub_segments", I64), ("row_tasks", I64), ("last_launches", I64)]
 
 
 class ZipView(ctypes.Structure):

@@ -29,6 +29,9 @@ namespace cola {
                                 "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, __LINE__);    \
     } while (0)
 
+// Kernel launches issued by this thread (cola_spmm reports the count of its last call).
+static thread_local int64_t t_launches = 0;
+
 static int sm_count()
 {
     static int cached[64] = {0};
@@ -102,6 +105,7 @@ static cola_status launch_fused_t(const FusedArgs &a, cudaStream_t st)
     auto fn = dev::fused_spmm_kernel<TR, LG, NV, UNROLL, VEC_Y>;
     const int64_t gx = grid_for((const void *)fn, a.total);
     const int gy = (a.K + W - 1) / W;
+    t_launches++;
     fn<<<dim3((unsigned)gx, (unsigned)gy), dev::kThreads, 0, st>>>(a.parts, a.single, a.nparts, a.total,
                                                                    static_cast<const T *>(a.X), a.ldx, a.Y, a.ldy,
                                                                    a.K);
@@ -174,6 +178,7 @@ static cola_status launch_gather(const GatherSeg *segs, const GatherSeg &single,
         using T = typename dev::ElemOf<TR>::T;                                                                 \
         auto fn = dev::gather_rows_kernel<TR>;                                                                 \
         const int64_t gx = grid_for((const void *)fn, total);                                                 \
+        t_launches++;                                                                                          \
         fn<<<(unsigned)gx, dev::kThreads, 0, st>>>(segs, single, nsegs, total, static_cast<const T *>(src),    \
                                                    ld_src, static_cast<T *>(dst), ld_dst, K);                 \
     } while (0)
@@ -218,6 +223,7 @@ static cola_status launch_rows_t(const RowsLaunch &a, cudaStream_t st)
     auto fn = dev::rows_spmm_kernel<TR, TY, LG, NV, UNROLL, VEC>;
     const int64_t gx = grid_for((const void *)fn, a.ra.nseg + a.ra.nrows);
     const int gy = (a.K + W - 1) / W;
+    t_launches++;
     fn<<<dim3((unsigned)gx, (unsigned)gy), dev::kThreads, 0, st>>>(a.ra, static_cast<const T *>(a.X), a.ldx,
                                                                    static_cast<TY *>(a.Y), a.ldy, a.K, a.accumulate);
     COLA_CUDA(cudaGetLastError());
@@ -279,6 +285,7 @@ static cola_status launch_block_t(const dev::BlockArgs &ba, const RowsLaunch &a,
     auto fn = dev::rowblock_spmm_kernel<TR, TY, NV, UNROLL, VEC, MINB>;
     const int64_t gx = grid_for((const void *)fn, ba.nseg + ba.ntask);
     const int gy = (a.K + W - 1) / W;
+    t_launches++;
     fn<<<dim3((unsigned)gx, (unsigned)gy), dev::kThreads, 0, st>>>(ba, static_cast<const T *>(a.X), a.ldx,
                                                                    static_cast<TY *>(a.Y), a.ldy, a.K, a.accumulate);
     COLA_CUDA(cudaGetLastError());
@@ -550,6 +557,7 @@ struct cola_graph {
     size_t stage_bytes = 0;
     float *ws = nullptr;  // FP32 accumulator for BF16 output
     size_t ws_bytes = 0;
+    int64_t last_launches = 0;       // kernels launched by the last cola_spmm call
     GatherSeg *d_bufsegs = nullptr;  // BUFFER schedule gather segments
     std::vector<GatherSeg> h_bufsegs;
     // row-major view (ROWS schedule): merged local + transposed remote entries
@@ -1014,6 +1022,7 @@ cola_status cola_graph_get_info(const cola_graph *g, cola_graph_info *o)
     o->hub_rows = g->nhub;
     o->hub_segments = g->nseg;
     o->row_tasks = g->ntask;
+    o->last_launches = g->last_launches;
     return COLA_SUCCESS;
 }
 
@@ -1025,8 +1034,21 @@ cola_status cola_graph_zip_view(const cola_graph *g, int32_t part, cola_zip_view
     return COLA_SUCCESS;
 }
 
+static cola_status spmm_impl(cola_graph *g, const void *X, cola_dtype xdt, int64_t ldx, void *Y, cola_dtype ydt,
+                             int64_t ldy, int32_t K, const cola_spmm_opts *opts, cola_stream_t stream);
+
 cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype xdt, int64_t ldx, void *Y, cola_dtype ydt,
                       int64_t ldy, int32_t K, const cola_spmm_opts *opts, cola_stream_t stream)
+{
+    const int64_t before = t_launches;
+    const cola_status s = spmm_impl(g, X, xdt, ldx, Y, ydt, ldy, K, opts, stream);
+    if (g)
+        g->last_launches = t_launches - before;
+    return s;
+}
+
+static cola_status spmm_impl(cola_graph *g, const void *X, cola_dtype xdt, int64_t ldx, void *Y, cola_dtype ydt,
+                             int64_t ldy, int32_t K, const cola_spmm_opts *opts, cola_stream_t stream)
 {
     COLA_REQUIRE(g, COLA_ERROR_INVALID_ARGUMENT, "cola_spmm: graph is NULL");
     COLA_REQUIRE(K >= 1 && ldx >= K && ldy >= K, COLA_ERROR_INVALID_ARGUMENT, "cola_spmm: K=%d ldx=%lld ldy=%lld",
@@ -1101,8 +1123,23 @@ cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype xdt, int64_t ldx,
         } else {
             COLA_TRY(launch_rows(a, st));
         }
-        if (g->nhub > 0) {
+        if (g->nhub > 0 && K % 4 == 0 && (ydt == COLA_FLOAT32 ? ldy % 4 == 0 : ldy % 4 == 0) &&
+            aligned16(g->ws_hub) && ((uintptr_t)Y % (ydt == COLA_FLOAT32 ? 16 : 8)) == 0) {
+            const int64_t items = g->nhub * ((K + 127) / 128);
+            const int64_t blocks = std::min<int64_t>((items + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock,
+                                                     (int64_t)sm_count() * 16);
+            t_launches++;
+            if (ydt == COLA_FLOAT32)
+                dev::hub_combine_vec_kernel<float, 4><<<(unsigned)blocks, dev::kThreads, 0, st>>>(
+                    g->hub_row, g->hub_seg, g->nhub, g->ws_hub, K, static_cast<float *>(Y), ldy, K, accumulate);
+            else
+                dev::hub_combine_vec_kernel<__nv_bfloat16, 4><<<(unsigned)blocks, dev::kThreads, 0, st>>>(
+                    g->hub_row, g->hub_seg, g->nhub, g->ws_hub, K, static_cast<__nv_bfloat16 *>(Y), ldy, K,
+                    accumulate);
+            COLA_CUDA(cudaGetLastError());
+        } else if (g->nhub > 0) {
             const int64_t blocks = (g->nhub + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock;
+            t_launches++;
             if (ydt == COLA_FLOAT32)
                 dev::hub_combine_kernel<float><<<(unsigned)blocks, dev::kThreads, 0, st>>>(
                     g->hub_row, g->hub_seg, g->nhub, g->ws_hub, K, static_cast<float *>(Y), ldy, K, accumulate);
@@ -1229,6 +1266,7 @@ cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype xdt, int64_t ldx,
     if (ydt == COLA_BFLOAT16) {
         const int64_t n = (int64_t)g->N * K;
         const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 8);
+        t_launches++;
         dev::f32_to_bf16_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), dev::kThreads, 0, st>>>(
             acc, ldacc, static_cast<__nv_bfloat16 *>(Y), ldy, g->N, K);
         COLA_CUDA(cudaGetLastError());

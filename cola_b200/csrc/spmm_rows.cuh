@@ -435,5 +435,65 @@ __global__ void __launch_bounds__(kThreads) hub_combine_kernel(const int32_t *__
     }
 }
 
+// Hub rows, 16-byte vector form (K a multiple of 4, ws rows 16-byte aligned):
+// one warp per (hub, 128-feature tile); every partial is read exactly once,
+// UNROLL partials in flight, and summed pairwise by a binary counter: partial
+// i is added to the running block sums of sizes 1, 2, 4, ... that its index's
+// trailing one bits close, so the sum is the same fixed binary tree for every
+// run.  The stack has one slot per tree level (at most 32).
+template <typename TY, int UNROLL>
+__global__ void __launch_bounds__(kThreads) hub_combine_vec_kernel(const int32_t *__restrict__ hub_row,
+                                                                  const int64_t *__restrict__ hub_seg, int64_t nhub,
+                                                                  const float *__restrict__ ws, int64_t ld_ws,
+                                                                  TY *__restrict__ Y, int64_t ldy, int K,
+                                                                  int accumulate)
+{
+    const int lane = threadIdx.x & 31;
+    const int tiles = (K + 127) / 128;
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    for (int64_t w = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); w < nhub * tiles; w += nwarps) {
+        const int64_t h = w / tiles;
+        const int k = (int)(w % tiles) * 128 + lane * 4;
+        const bool kok = k < K;
+        const int64_t s0 = __ldg(hub_seg + h), m = __ldg(hub_seg + h + 1) - s0;
+        const float *wp = ws + s0 * ld_ws + k;
+        float4 stk[32];
+        for (int64_t i0 = 0; i0 < m; i0 += UNROLL) {
+            float4 v[UNROLL];
+#pragma unroll
+            for (int u = 0; u < UNROLL; u++)
+                if (kok && i0 + u < m)
+                    v[u] = __ldcg(reinterpret_cast<const float4 *>(wp + (i0 + u) * ld_ws));
+#pragma unroll
+            for (int u = 0; u < UNROLL; u++) {
+                const int64_t i = i0 + u;
+                if (i < m) {
+                    float4 c = v[u];
+                    int l = 0;
+                    while ((i >> l) & 1) {
+                        const float4 a = stk[l];
+                        c = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w + c.w);
+                        l++;
+                    }
+                    stk[l] = c;
+                }
+            }
+        }
+        // fold the open block sums, larger (earlier) blocks first
+        float4 tot = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool first = true;
+        for (int l = 31; l >= 0; l--)
+            if ((m >> l) & 1) {
+                const float4 a = stk[l];
+                tot = first ? a : make_float4(tot.x + a.x, tot.y + a.y, tot.z + a.z, tot.w + a.w);
+                first = false;
+            }
+        if (kok) {
+            const float r[4] = {tot.x, tot.y, tot.z, tot.w};
+            store_out<TY, 4, true>(Y + (int64_t)__ldg(hub_row + h) * ldy + k, r, accumulate != 0);
+        }
+    }
+}
+
 }  // namespace dev
 }  // namespace cola

@@ -271,6 +271,7 @@ typedef struct cola_graph_info {
     int64_t device_bytes;
     int64_t hub_rows, hub_segments;  /* ROWS schedule */
     int64_t row_tasks;               /* ROWS schedule: row blocks of about task_entries entries */
+    int64_t last_launches;           /* kernels the last cola_spmm call on this graph launched */
 } cola_graph_info;
 cola_status cola_graph_get_info(const cola_graph *g, cola_graph_info *out);
 

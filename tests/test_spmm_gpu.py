@@ -417,3 +417,22 @@ def test_rows_view_optional(case12):
     Y = g.spmm(torch.ones((n, 16), device=DEV))  # AUTO falls back to the fused schedule
     torch.cuda.synchronize()
     assert Y.shape == (n, 16)
+
+
+@pytest.mark.parametrize("K,thr,seg", [(128, 16, 8), (1024, 32, 16), (256, 1, 1)])
+def test_rows_hub_combine_tiles_and_repeats(case12, K, thr, seg):
+    """Hub rows: segment partials from the streaming kernel, combined pairwise
+    by the vector combine kernel -- right on every call, over several feature
+    tiles (K = 1024 FP32 is two tiles), two launches per call."""
+    n, row, col, val, ps = case12
+    g = S.Graph(ps, hub_threshold=thr, hub_segment=seg)
+    assert g.info.hub_rows > 0
+    X = dense_x(n, K, seed=K + thr)
+    ref = fp64_reference(n, row, col, val, X)
+    xt = torch.from_numpy(X).to(DEV)
+    outs = [g.spmm(xt, schedule=S.SCHEDULE_ROWS) for _ in range(3)]
+    torch.cuda.synchronize()
+    assert g.get_info().last_launches == 2
+    for y in outs:
+        assert rel(y.cpu().numpy(), ref) <= TOL_F32
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[1], outs[2])
