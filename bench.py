@@ -378,7 +378,7 @@ def run_ours(args, w):
     achieved = B / (k_ms * 1e-3) / 1e9
     traffic = read_traffic({"fp32": "rowblock_spmm_rmat20_k128_fp32.md", "bf16": "rowblock_spmm_rmat21_k256_bf16.md",
                             "fp32-k256": "rowblock_spmm_rmat21_k256_fp32.md"}[args.workload]) \
-        if eff == S.SCHEDULE_ROWS and args.scale is None else None
+        if eff == S.SCHEDULE_ROWS and args.scale is None and args.K is None else None
     launches_per_step = int(g.get_info().last_launches)  # counted by the library
     line = {
         "metric": METRIC, "value": B * world / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world,
@@ -447,11 +447,15 @@ def main():
     ap.add_argument("--task-entries", type=int, default=0, help="row-major schedule: entries per row-block task")
     ap.add_argument("--min-blocks", type=int, default=0, help="row-major schedule: resident blocks per SM")
     ap.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
+    ap.add_argument("--K", type=int, default=None, help="override the feature width (exploration runs)")
     args = ap.parse_args()
     w = dict(WORKLOADS[args.workload])
     if args.scale is not None:
         w["scale"] = args.scale
         w["desc"] = "{} [scale overridden to {}]".format(w["desc"], args.scale)
+    if args.K is not None:
+        w["K"] = args.K
+        w["desc"] = "{} [K overridden to {}]".format(w["desc"], args.K)
     if args.impl == "reference":
         return run_reference(args, w)
     return run_ours(args, w)

@@ -277,12 +277,12 @@ static cola_status launch_rows(const RowsLaunch &a, cudaStream_t st)
                  : launch_rows_geo<dev::ScalarTraits<BF>, BF, false>(a, a.K, st);
 }
 
-template <typename TR, typename TY, int NV, int UNROLL, bool VEC, int MINB = 1>
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC, int MINB = 1>
 static cola_status launch_block_t(const dev::BlockArgs &ba, const RowsLaunch &a, cudaStream_t st)
 {
     using T = typename dev::ElemOf<TR>::T;
-    constexpr int W = 32 * NV * TR::E;
-    auto fn = dev::rowblock_spmm_kernel<TR, TY, NV, UNROLL, VEC, MINB>;
+    constexpr int W = LG * NV * TR::E;
+    auto fn = dev::rowblock_spmm_kernel<TR, TY, LG, NV, UNROLL, VEC, MINB>;
     const int64_t gx = grid_for((const void *)fn, ba.nseg + ba.ntask);
     const int gy = (a.K + W - 1) / W;
     t_launches++;
@@ -292,33 +292,44 @@ static cola_status launch_block_t(const dev::BlockArgs &ba, const RowsLaunch &a,
     return COLA_SUCCESS;
 }
 
+// V = 16-byte vectors per row: LG lanes per row tile, G = 32/LG lane groups.
 template <typename TR, typename TY>
 static cola_status launch_block_geo(const dev::BlockArgs &ba, const RowsLaunch &a, int V, cudaStream_t st)
 {
+    if (V <= 1)
+        return launch_block_t<TR, TY, 1, 1, 1, true>(ba, a, st);
+    if (V <= 2)
+        return launch_block_t<TR, TY, 2, 1, 2, true>(ba, a, st);
+    if (V <= 4)
+        return launch_block_t<TR, TY, 4, 1, 4, true, 4>(ba, a, st);
+    if (V <= 8)
+        return launch_block_t<TR, TY, 8, 1, 4, true, 4>(ba, a, st);
+    if (V <= 16)
+        return launch_block_t<TR, TY, 16, 1, 4, true, 4>(ba, a, st);
     if (V <= 32) {
         if (a.unroll == 8)
-            return launch_block_t<TR, TY, 1, 8, true>(ba, a, st);
+            return launch_block_t<TR, TY, 32, 1, 8, true>(ba, a, st);
         if (a.unroll == 2)
-            return launch_block_t<TR, TY, 1, 2, true>(ba, a, st);
+            return launch_block_t<TR, TY, 32, 1, 2, true>(ba, a, st);
         if (a.unroll == 6)
-            return launch_block_t<TR, TY, 1, 6, true>(ba, a, st);
+            return launch_block_t<TR, TY, 32, 1, 6, true>(ba, a, st);
         if (a.min_blocks == 3)
-            return launch_block_t<TR, TY, 1, 4, true, 3>(ba, a, st);
+            return launch_block_t<TR, TY, 32, 1, 4, true, 3>(ba, a, st);
         if (a.min_blocks == 5)
-            return launch_block_t<TR, TY, 1, 4, true, 5>(ba, a, st);
+            return launch_block_t<TR, TY, 32, 1, 4, true, 5>(ba, a, st);
         if (a.min_blocks == 6)
-            return launch_block_t<TR, TY, 1, 4, true, 6>(ba, a, st);
-        return launch_block_t<TR, TY, 1, 4, true, 4>(ba, a, st);
+            return launch_block_t<TR, TY, 32, 1, 4, true, 6>(ba, a, st);
+        return launch_block_t<TR, TY, 32, 1, 4, true, 4>(ba, a, st);
     }
     if (V <= 64) {
         if (a.unroll == 4 || a.unroll == 8)
-            return launch_block_t<TR, TY, 2, 4, true>(ba, a, st);
-        return launch_block_t<TR, TY, 2, 2, true>(ba, a, st);
+            return launch_block_t<TR, TY, 32, 2, 4, true>(ba, a, st);
+        return launch_block_t<TR, TY, 32, 2, 2, true>(ba, a, st);
     }
-    return launch_block_t<TR, TY, 4, 2, true>(ba, a, st);
+    return launch_block_t<TR, TY, 32, 4, 2, true>(ba, a, st);
 }
 
-// Row-block streaming launch for rows one warp wide (vector path, V > 16).
+// Row-block streaming launch (vector path).
 static cola_status launch_block(const dev::BlockArgs &ba, const RowsLaunch &a, cudaStream_t st)
 {
     if (ba.nseg + ba.ntask <= 0)
@@ -1105,7 +1116,7 @@ static cola_status spmm_impl(cola_graph *g, const void *X, cola_dtype xdt, int64
         a.unroll = opts ? opts->unroll : 0;
         a.min_blocks = opts ? opts->min_blocks : 0;
         const int V = a.vec ? K / (xdt == COLA_FLOAT32 ? 4 : 8) : 0;
-        if (a.vec && V > 16) {
+        if (a.vec) {
             dev::BlockArgs ba;
             ba.rowptr = g->rv_ptr;
             ba.col = g->rv_col;
@@ -1123,7 +1134,7 @@ static cola_status spmm_impl(cola_graph *g, const void *X, cola_dtype xdt, int64
         } else {
             COLA_TRY(launch_rows(a, st));
         }
-        if (g->nhub > 0 && K % 4 == 0 && (ydt == COLA_FLOAT32 ? ldy % 4 == 0 : ldy % 4 == 0) &&
+        if (g->nhub > 0 && a.vec && K % 4 == 0 && ldy % 4 == 0 &&
             aligned16(g->ws_hub) && ((uintptr_t)Y % (ydt == COLA_FLOAT32 ? 16 : 8)) == 0) {
             const int64_t items = g->nhub * ((K + 127) / 128);
             const int64_t blocks = std::min<int64_t>((items + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock,

@@ -238,7 +238,14 @@ __device__ __forceinline__ void fma_vec2(float2 (&acc)[TR::E / 2], float v, cons
         acc[q] = __ffma2_rn(vv, make_float2(f[2 * q], f[2 * q + 1]), acc[q]);
 }
 
-template <typename TR, typename TY, int NV, int UNROLL, bool VEC_Y, int MINB = 1>
+// LG lanes cover one row tile of X (NV vectors each); G = 32 / LG lane groups
+// of the warp take interleaved entries of the same stream (group g takes
+// entries g, g + G, ...), so narrow rows still keep 32 lanes busy.  A round is
+// G * UNROLL consecutive entries: when it lies inside the current output row
+// every group just accumulates; otherwise it is cut at the row ends, and at
+// every row end the groups' partial sums are added with __shfl_xor_sync and
+// group 0 writes the row.
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, int MINB = 1>
 __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __grid_constant__ BlockArgs ba,
                                                                        const typename ElemOf<TR>::T *__restrict__ X,
                                                                        int64_t ldx, TY *__restrict__ Y, int64_t ldy,
@@ -247,20 +254,25 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
     using T = typename ElemOf<TR>::T;
     using raw_t = typename TR::raw_t;
     constexpr int E = TR::E;
-    constexpr int W = 32 * NV * E;
-    // the current batch of 32 (col, val) pairs of each warp, read back as
-    // one 8-byte broadcast load per entry
+    constexpr int G = 32 / LG;
+    constexpr int R = G * UNROLL;  // entries per round
+    static_assert(R <= 32, "a round must fit in the 32-entry index batch");
+    constexpr int W = LG * NV * E;
+    // the current batch of 32 (col, val) pairs of each warp, read back with
+    // one 8-byte shared-memory load per entry and lane group
     __shared__ int2 s_ent[kWarpsPerBlock][32];
     int2 *ent = s_ent[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
+    const int g = lane / LG;
+    const int gl = lane % LG;
     const int k0 = blockIdx.y * W;
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
     const int64_t total = ba.nseg + ba.ntask;
     bool kok[NV];
 #pragma unroll
     for (int j = 0; j < NV; j++)
-        kok[j] = (k0 + (lane + j * 32) * E) < K;
-    const T *xk = X + k0 + lane * E;
+        kok[j] = (k0 + (gl + j * LG) * E) < K;
+    const T *xk = X + k0 + gl * E;
 
     for (int64_t it = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); it < total; it += nwarps) {
         const bool seg = it < ba.nseg;
@@ -295,30 +307,41 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
                 acc[j][q] = make_float2(0.f, 0.f);
 
         auto flush = [&]() {
-            if (seg) {
-                float *wp = ba.ws + it * ba.ld_ws + k0 + lane * E;
+#pragma unroll
+            for (int off = LG; off < 32; off <<= 1)
 #pragma unroll
                 for (int j = 0; j < NV; j++)
-                    if (kok[j]) {
 #pragma unroll
-                        for (int q = 0; q < E / 2; q++) {
-                            wp[j * 32 * E + 2 * q] = acc[j][q].x;
-                            wp[j * 32 * E + 2 * q + 1] = acc[j][q].y;
-                        }
+                    for (int q = 0; q < E / 2; q++) {
+                        acc[j][q].x += __shfl_xor_sync(kFull, acc[j][q].x, off);
+                        acc[j][q].y += __shfl_xor_sync(kFull, acc[j][q].y, off);
                     }
-            } else {
-                TY *yp = Y + (int64_t)cur * ldy + k0 + lane * E;
+            if (g == 0) {
+                if (seg) {
+                    float *wp = ba.ws + it * ba.ld_ws + k0 + gl * E;
 #pragma unroll
-                for (int j = 0; j < NV; j++)
-                    if (kok[j]) {
-                        float a[E];
+                    for (int j = 0; j < NV; j++)
+                        if (kok[j]) {
 #pragma unroll
-                        for (int q = 0; q < E / 2; q++) {
-                            a[2 * q] = acc[j][q].x;
-                            a[2 * q + 1] = acc[j][q].y;
+                            for (int q = 0; q < E / 2; q++) {
+                                wp[j * LG * E + 2 * q] = acc[j][q].x;
+                                wp[j * LG * E + 2 * q + 1] = acc[j][q].y;
+                            }
                         }
-                        store_out<TY, E, VEC_Y>(yp + j * 32 * E, a, accumulate != 0);
-                    }
+                } else {
+                    TY *yp = Y + (int64_t)cur * ldy + k0 + gl * E;
+#pragma unroll
+                    for (int j = 0; j < NV; j++)
+                        if (kok[j]) {
+                            float a[E];
+#pragma unroll
+                            for (int q = 0; q < E / 2; q++) {
+                                a[2 * q] = acc[j][q].x;
+                                a[2 * q + 1] = acc[j][q].y;
+                            }
+                            store_out<TY, E, VEC_Y>(yp + j * LG * E, a, accumulate != 0);
+                        }
+                }
             }
 #pragma unroll
             for (int j = 0; j < NV; j++)
@@ -351,21 +374,20 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
                 mc = __ldg(colp + base + 32 + lane);
                 mv = __ldg(valp + base + 32 + lane);
             }
-            for (int jj = 0; jj < n; jj += UNROLL) {
-                const int32_t e0 = base + jj;
+            for (int jj = 0; jj < n; jj += R) {
                 raw_t xr[UNROLL][NV];
                 float vv[UNROLL];
-                if (jj + UNROLL <= n && e0 + UNROLL <= row_end) {
-                    // whole group inside the current row: no boundary checks
+                if (jj + R <= n && base + jj + R <= row_end) {
+                    // the whole round inside the current row: no boundary checks
 #pragma unroll
                     for (int u = 0; u < UNROLL; u++) {
-                        const int2 p = ent[jj + u];
+                        const int2 p = ent[jj + u * G + g];
                         vv[u] = __int_as_float(p.y);
                         const T *xp = xk + (int64_t)p.x * ldx;
 #pragma unroll
                         for (int j = 0; j < NV; j++)
                             if (kok[j])
-                                xr[u][j] = TR::load(xp + j * 32 * E);
+                                xr[u][j] = TR::load(xp + j * LG * E);
                     }
 #pragma unroll
                     for (int u = 0; u < UNROLL; u++)
@@ -375,25 +397,36 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
                 } else {
 #pragma unroll
                     for (int u = 0; u < UNROLL; u++) {
-                        if (jj + u < n) {
-                            const int2 p = ent[jj + u];
+                        const int idx = jj + u * G + g;
+                        if (idx < n) {
+                            const int2 p = ent[idx];
                             vv[u] = __int_as_float(p.y);
                             const T *xp = xk + (int64_t)p.x * ldx;
 #pragma unroll
                             for (int j = 0; j < NV; j++)
                                 if (kok[j])
-                                    xr[u][j] = TR::load(xp + j * 32 * E);
+                                    xr[u][j] = TR::load(xp + j * LG * E);
                         }
                     }
+                    // cut the round [lo, hi) at the row ends it contains
+                    int32_t lo = base + jj;
+                    const int32_t hi = base + jj + min(R, n - jj);
+                    while (true) {
+                        while (lo >= row_end)
+                            flush();
+                        const int32_t sh = min(row_end, hi);
 #pragma unroll
-                    for (int u = 0; u < UNROLL; u++) {
-                        if (jj + u < n) {
-                            while (e0 + u >= row_end)
-                                flush();
+                        for (int u = 0; u < UNROLL; u++) {
+                            const int32_t e = base + jj + u * G + g;
+                            if (e >= lo && e < sh) {
 #pragma unroll
-                            for (int j = 0; j < NV; j++)
-                                fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
+                                for (int j = 0; j < NV; j++)
+                                    fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
+                            }
                         }
+                        lo = sh;
+                        if (lo >= hi)
+                            break;
                     }
                 }
             }
