@@ -69,6 +69,11 @@ class SpmmOpts(ctypes.Structure):
                 ("min_blocks", I32), ("reserved", I32 * 3)]
 
 
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("ngraphs", I32), ("batched_graphs", I32), ("work_items", I64), ("hub_items", I64),
+                ("nnz", I64), ("device_bytes", I64), ("unroll", I32), ("grid_pct", I32), ("last_launches", I64)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "cola_status_string": (ctypes.c_char_p, [I32]),
@@ -99,6 +104,15 @@ SIGNATURES = {
     "cola_graph_get_info": (I32, [P, P]),
     "cola_graph_zip_view": (I32, [P, I32, P]),
     "cola_spmm": (I32, [P, P, I32, I64, P, I32, I64, I32, P, P]),
+    "cola_batch_create": (I32, [P, I32, P, P, P]),
+    "cola_batch_free": (I32, [P]),
+    "cola_batch_bind": (I32, [P, P, P, P, P, P, I32, I32, P]),
+    "cola_batch_run": (I32, [P, P, P]),
+    "cola_batch_capture": (I32, [P, P, P]),
+    "cola_batch_replay": (I32, [P, P]),
+    "cola_batch_set_params": (I32, [P, I32, I32]),
+    "cola_batch_autotune": (I32, [P, I32, P, P]),
+    "cola_batch_get_info": (I32, [P, P]),
 }
 
 _lib = None

@@ -13,6 +13,7 @@
 
 #include "common.h"
 #include "prep.h"
+#include "graph.h"
 #include "spmm_kernels.cuh"
 #include "spmm_rows.cuh"
 
@@ -21,18 +22,11 @@ using cola::dev::PartDesc;
 
 namespace cola {
 
-#define COLA_CUDA(expr)                                                                                   \
-    do {                                                                                                  \
-        cudaError_t _e = (expr);                                                                          \
-        if (_e != cudaSuccess)                                                                            \
-            return ::cola::fail(_e == cudaErrorMemoryAllocation ? COLA_ERROR_OUT_OF_MEMORY : COLA_ERROR_CUDA, \
-                                "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, __LINE__);    \
-    } while (0)
 
 // Kernel launches issued by this thread (cola_spmm reports the count of its last call).
-static thread_local int64_t t_launches = 0;
+thread_local int64_t t_launches = 0;
 
-static int sm_count()
+int sm_count()
 {
     static int cached[64] = {0};
     int dev = 0;
@@ -48,7 +42,7 @@ static int sm_count()
 }
 
 // Resident blocks per SM for a kernel (cached by function address).
-static int blocks_per_sm(const void *fn, int threads)
+int blocks_per_sm(const void *fn, int threads)
 {
     static std::mutex mu;
     static std::unordered_map<const void *, int> cache;
@@ -63,14 +57,13 @@ static int blocks_per_sm(const void *fn, int threads)
     return n;
 }
 
-static int64_t grid_for(const void *fn, int64_t items)
+int64_t grid_for(const void *fn, int64_t items)
 {
     const int64_t need = (items + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock;
     const int64_t full = (int64_t)sm_count() * blocks_per_sm(fn, dev::kThreads);
     return std::max<int64_t>(1, std::min(need, full));
 }
 
-static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 
 static int next_pow2(int v)
 {
@@ -344,7 +337,7 @@ static cola_status launch_block(const dev::BlockArgs &ba, const RowsLaunch &a, c
 
 // Vector path of the row-major schedule: X rows in 16-byte vectors, Y rows
 // written E elements at a time (E*sizeof(TY) bytes, aligned).
-static bool vec_ok_rows(cola_dtype xdt, const void *X, int64_t ldx, cola_dtype ydt, const void *Y, int64_t ldy, int K)
+bool vec_ok_rows(cola_dtype xdt, const void *X, int64_t ldx, cola_dtype ydt, const void *Y, int64_t ldy, int K)
 {
     const int E = xdt == COLA_FLOAT32 ? 4 : 8;
     const int ysz = ydt == COLA_FLOAT32 ? 4 : 2;
@@ -540,56 +533,10 @@ cola_status cola_batching_data_ppl(const float *input, float *send, const int32_
 // ===========================================================================
 // Device-resident graph
 // ===========================================================================
-struct cola_graph {
-    int device = 0;
-    int32_t N = 0, P = 0, npp = 0, gs = 0, nstages = 1, if_split = 1;
-    int64_t nnz_l = 0, nnz_r = 0, lchunks = 0, rchunks = 0, rcols = 0;
-    void *dmem = nullptr;
-    size_t dbytes = 0;
-    std::vector<cola_zip_view> zips;
-    // fused schedule: all parts, all chunks
-    PartDesc *d_fused = nullptr;
-    int64_t fused_total = 0;
-    std::vector<PartDesc> h_fused;
-    // pipelined schedule (group_size < P)
-    std::vector<cola::StageTables> tables;
-    PartDesc *d_stage0 = nullptr;  // local + intra-group remote of every PE
-    int64_t stage0_total = 0;
-    std::vector<PartDesc *> d_stage;  // stage s >= 1 (index s-1), mode 2
-    std::vector<int64_t> stage_total;
-    std::vector<std::vector<PartDesc>> h_stage;
-    std::vector<GatherSeg *> d_put;  // puts feeding stage s (index s-1)
-    std::vector<int64_t> put_total;
-    std::vector<std::vector<GatherSeg>> h_put;
-    // lazily sized workspaces
-    void *ppl_buf = nullptr;  // 2 x P x npp x K elements
-    size_t ppl_bytes = 0;
-    void *stage_buf = nullptr;  // BUFFER schedule staging
-    size_t stage_bytes = 0;
-    float *ws = nullptr;  // FP32 accumulator for BF16 output
-    size_t ws_bytes = 0;
-    int64_t last_launches = 0;       // kernels launched by the last cola_spmm call
-    GatherSeg *d_bufsegs = nullptr;  // BUFFER schedule gather segments
-    std::vector<GatherSeg> h_bufsegs;
-    // row-major view (ROWS schedule): merged local + transposed remote entries
-    bool has_rows = false;
-    const int64_t *rv_ptr = nullptr;  // N+1
-    const int32_t *rv_col = nullptr;
-    const float *rv_val = nullptr;
-    const int32_t *seg_row = nullptr;
-    const int64_t *seg_beg = nullptr;
-    const int32_t *hub_row = nullptr;
-    const int64_t *hub_seg = nullptr;
-    const int32_t *task_rb = nullptr, *task_re = nullptr;
-    int64_t nseg = 0, nhub = 0, ntask = 0;
-    int32_t hub_threshold = 256, hub_segment = 256, task_entries = 256;
-    float *ws_hub = nullptr;  // nseg x K partials
-    size_t ws_hub_bytes = 0;
-};
 
 namespace cola {
 
-static cola_status ensure(void *&p, size_t &have, size_t need)
+cola_status ensure(void *&p, size_t &have, size_t need)
 {
     if (have >= need)
         return COLA_SUCCESS;
@@ -602,7 +549,7 @@ static cola_status ensure(void *&p, size_t &have, size_t need)
     return COLA_SUCCESS;
 }
 
-static void graph_release(cola_graph *g)
+void graph_release(cola_graph *g)
 {
     if (!g)
         return;
@@ -633,7 +580,7 @@ struct Arena {
     }
 };
 
-static cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *opts, cola_graph *&out,
+cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *opts, cola_graph *&out,
                                 cudaStream_t st)
 {
     COLA_REQUIRE(ps, COLA_ERROR_INVALID_ARGUMENT, "cola_graph_upload: partition set is NULL");

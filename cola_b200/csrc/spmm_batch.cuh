@@ -1,0 +1,75 @@
+// Batched form: many graphs, each with its own X, Y and feature width, in one
+// persistent launch.  Work items of all graphs are concatenated (graph g owns
+// items [item0, item0 + nseg + ntask)); a warp finds its graph by advancing
+// through the descriptor table (its items only increase) and runs the item with
+// the lane geometry of that graph's width.
+#pragma once
+#include "spmm_rows.cuh"
+
+namespace cola {
+namespace dev {
+
+struct BatchGraph {
+    BlockArgs ba;  // row view, tasks, hub segments, workspace of this graph
+    const void *X;
+    int64_t ldx;
+    void *Y;
+    int64_t ldy;
+    int32_t K;
+    int32_t lg;    // reserved
+    int64_t item0; // first work item of this graph in the launch
+    int64_t hub0;  // first combine item (hub x 128-feature tile) of this graph
+    const int32_t *hub_row;
+    const int64_t *hub_seg;
+    int64_t nhub;
+};
+
+// Every graph runs with the same lane geometry: 8 lanes cover one 128-byte
+// line of an X row (32 FP32 or 64 BF16 features) and the warp's 4 lane groups
+// take interleaved entries, so one warp load instruction fetches 4 lines.  A
+// task walks its graph's feature tiles one after the other (the index batch is
+// re-read from cache per tile; X bytes per entry do not change), so graphs of
+// any width share the one kernel.
+constexpr int kBatchLG = 8;
+
+template <typename TR, typename TY, int UNROLL>
+__global__ void __launch_bounds__(kThreads, 4) batch_rowblock_kernel(const BatchGraph *__restrict__ gs, int ng,
+                                                                     int64_t total, int accumulate)
+{
+    using T = typename ElemOf<TR>::T;
+    constexpr int W = kBatchLG * TR::E;  // features per tile
+    __shared__ int2 s_ent[kWarpsPerBlock][32];
+    int2 *ent = s_ent[threadIdx.x >> 5];
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    int gi = 0;
+    for (int64_t it = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); it < total; it += nwarps) {
+        while (gi + 1 < ng && it >= gs[gi + 1].item0)
+            gi++;
+        const BatchGraph &bg = gs[gi];
+        const int64_t li = it - bg.item0;
+        for (int k0 = 0; k0 < bg.K; k0 += W)
+            rowblock_item<TR, TY, kBatchLG, 1, UNROLL, true>(bg.ba, li, static_cast<const T *>(bg.X), bg.ldx,
+                                                             static_cast<TY *>(bg.Y), bg.ldy, bg.K, accumulate, k0,
+                                                             ent);
+    }
+}
+
+template <typename TY, int UNROLL>
+__global__ void __launch_bounds__(kThreads) batch_hub_combine_kernel(const BatchGraph *__restrict__ gs, int ng,
+                                                                    int64_t total, int accumulate)
+{
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    int gi = 0;
+    for (int64_t w = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); w < total; w += nwarps) {
+        while (gi + 1 < ng && w >= gs[gi + 1].hub0)
+            gi++;
+        const BatchGraph &bg = gs[gi];
+        const int tiles = (bg.K + 127) / 128;
+        const int64_t lw = w - bg.hub0;
+        hub_combine_item<TY, UNROLL>(bg.hub_row, bg.hub_seg, lw / tiles, (int)(lw % tiles), bg.ba.ws, bg.ba.ld_ws,
+                                     static_cast<TY *>(bg.Y), bg.ldy, bg.K, accumulate);
+    }
+}
+
+}  // namespace dev
+}  // namespace cola

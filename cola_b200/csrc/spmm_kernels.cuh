@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(kThreads) gather_rows_kernel(const GatherSeg *
 }
 
 // FP32 -> BF16 (round to nearest even) of an n x K block, row strides ld_in/ld_out.
-__global__ void __launch_bounds__(kThreads) f32_to_bf16_kernel(const float *__restrict__ in, int64_t ld_in,
+static __global__ void __launch_bounds__(kThreads) f32_to_bf16_kernel(const float *__restrict__ in, int64_t ld_in,
                                                               __nv_bfloat16 *__restrict__ out, int64_t ld_out,
                                                               int64_t rows, int K)
 {

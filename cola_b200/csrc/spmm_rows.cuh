@@ -245,11 +245,15 @@ __device__ __forceinline__ void fma_vec2(float2 (&acc)[TR::E / 2], float v, cons
 // every group just accumulates; otherwise it is cut at the row ends, and at
 // every row end the groups' partial sums are added with __shfl_xor_sync and
 // group 0 writes the row.
-template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, int MINB = 1>
-__global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __grid_constant__ BlockArgs ba,
-                                                                       const typename ElemOf<TR>::T *__restrict__ X,
-                                                                       int64_t ldx, TY *__restrict__ Y, int64_t ldy,
-                                                                       int K, int accumulate)
+// One work item of the streaming schedule: a row-block task (rows
+// [task_rb, task_re) of ba) or a hub segment (its partial goes to ws row `it`).
+// `it` counts segments first, then tasks.  k0 is the first feature of this
+// call's tile; ent is the warp's 32-entry shared-memory index batch.
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y>
+__device__ __forceinline__ void rowblock_item(const BlockArgs &ba, const int64_t it,
+                                              const typename ElemOf<TR>::T *__restrict__ X, const int64_t ldx,
+                                              TY *__restrict__ Y, const int64_t ldy, const int K, const int accumulate,
+                                              const int k0, int2 *ent)
 {
     using T = typename ElemOf<TR>::T;
     using raw_t = typename TR::raw_t;
@@ -257,131 +261,140 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
     constexpr int G = 32 / LG;
     constexpr int R = G * UNROLL;  // entries per round
     static_assert(R <= 32, "a round must fit in the 32-entry index batch");
-    constexpr int W = LG * NV * E;
-    // the current batch of 32 (col, val) pairs of each warp, read back with
-    // one 8-byte shared-memory load per entry and lane group
-    __shared__ int2 s_ent[kWarpsPerBlock][32];
-    int2 *ent = s_ent[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int g = lane / LG;
     const int gl = lane % LG;
-    const int k0 = blockIdx.y * W;
-    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
-    const int64_t total = ba.nseg + ba.ntask;
     bool kok[NV];
 #pragma unroll
     for (int j = 0; j < NV; j++)
         kok[j] = (k0 + (gl + j * LG) * E) < K;
     const T *xk = X + k0 + gl * E;
 
-    for (int64_t it = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); it < total; it += nwarps) {
-        const bool seg = it < ba.nseg;
-        int32_t rb, re;
-        int64_t e_beg;
-        int32_t n_ent;  // entries of this item; indices below are relative to e_beg
-        if (seg) {
-            rb = __ldg(ba.seg_row + it);
-            re = rb + 1;
-            e_beg = __ldg(ba.seg_beg + it);
-            n_ent = (int32_t)min((int64_t)ba.seg_len, __ldg(ba.rowptr + rb + 1) - e_beg);
-        } else {
-            const int64_t t = it - ba.nseg;
-            rb = __ldg(ba.task_rb + t);
-            re = __ldg(ba.task_re + t);
-            e_beg = __ldg(ba.rowptr + rb);
-            n_ent = (int32_t)(__ldg(ba.rowptr + re) - e_beg);
-        }
-        const int32_t *colp = ba.col + e_beg;
-        const float *valp = ba.val + e_beg;
-        // ends of rows q0 .. q0+31, relative to e_beg (lane l: row q0 + l)
-        int32_t q0 = rb;
-        int32_t my_end = seg ? n_ent : (rb + lane < re ? (int32_t)(__ldg(ba.rowptr + rb + lane + 1) - e_beg) : n_ent);
-        int32_t cur = rb;
-        int32_t row_end = __shfl_sync(kFull, my_end, 0);
+    const bool seg = it < ba.nseg;
+    int32_t rb, re;
+    int64_t e_beg;
+    int32_t n_ent;  // entries of this item; indices below are relative to e_beg
+    if (seg) {
+        rb = __ldg(ba.seg_row + it);
+        re = rb + 1;
+        e_beg = __ldg(ba.seg_beg + it);
+        n_ent = (int32_t)min((int64_t)ba.seg_len, __ldg(ba.rowptr + rb + 1) - e_beg);
+    } else {
+        const int64_t t = it - ba.nseg;
+        rb = __ldg(ba.task_rb + t);
+        re = __ldg(ba.task_re + t);
+        e_beg = __ldg(ba.rowptr + rb);
+        n_ent = (int32_t)(__ldg(ba.rowptr + re) - e_beg);
+    }
+    const int32_t *colp = ba.col + e_beg;
+    const float *valp = ba.val + e_beg;
+    // ends of rows q0 .. q0+31, relative to e_beg (lane l: row q0 + l)
+    int32_t q0 = rb;
+    int32_t my_end = seg ? n_ent : (rb + lane < re ? (int32_t)(__ldg(ba.rowptr + rb + lane + 1) - e_beg) : n_ent);
+    int32_t cur = rb;
+    int32_t row_end = __shfl_sync(kFull, my_end, 0);
 
-        float2 acc[NV][E / 2];
+    float2 acc[NV][E / 2];
+#pragma unroll
+    for (int j = 0; j < NV; j++)
+#pragma unroll
+        for (int q = 0; q < E / 2; q++)
+            acc[j][q] = make_float2(0.f, 0.f);
+
+    auto flush = [&]() {
+#pragma unroll
+        for (int off = LG; off < 32; off <<= 1)
+#pragma unroll
+            for (int j = 0; j < NV; j++)
+#pragma unroll
+                for (int q = 0; q < E / 2; q++) {
+                    acc[j][q].x += __shfl_xor_sync(kFull, acc[j][q].x, off);
+                    acc[j][q].y += __shfl_xor_sync(kFull, acc[j][q].y, off);
+                }
+        if (g == 0) {
+            if (seg) {
+                float *wp = ba.ws + it * ba.ld_ws + k0 + gl * E;
+#pragma unroll
+                for (int j = 0; j < NV; j++)
+                    if (kok[j]) {
+#pragma unroll
+                        for (int q = 0; q < E / 2; q++) {
+                            wp[j * LG * E + 2 * q] = acc[j][q].x;
+                            wp[j * LG * E + 2 * q + 1] = acc[j][q].y;
+                        }
+                    }
+            } else {
+                TY *yp = Y + (int64_t)cur * ldy + k0 + gl * E;
+#pragma unroll
+                for (int j = 0; j < NV; j++)
+                    if (kok[j]) {
+                        float a[E];
+#pragma unroll
+                        for (int q = 0; q < E / 2; q++) {
+                            a[2 * q] = acc[j][q].x;
+                            a[2 * q + 1] = acc[j][q].y;
+                        }
+                        store_out<TY, E, VEC_Y>(yp + j * LG * E, a, accumulate != 0);
+                    }
+            }
+        }
 #pragma unroll
         for (int j = 0; j < NV; j++)
 #pragma unroll
             for (int q = 0; q < E / 2; q++)
                 acc[j][q] = make_float2(0.f, 0.f);
-
-        auto flush = [&]() {
-#pragma unroll
-            for (int off = LG; off < 32; off <<= 1)
-#pragma unroll
-                for (int j = 0; j < NV; j++)
-#pragma unroll
-                    for (int q = 0; q < E / 2; q++) {
-                        acc[j][q].x += __shfl_xor_sync(kFull, acc[j][q].x, off);
-                        acc[j][q].y += __shfl_xor_sync(kFull, acc[j][q].y, off);
-                    }
-            if (g == 0) {
-                if (seg) {
-                    float *wp = ba.ws + it * ba.ld_ws + k0 + gl * E;
-#pragma unroll
-                    for (int j = 0; j < NV; j++)
-                        if (kok[j]) {
-#pragma unroll
-                            for (int q = 0; q < E / 2; q++) {
-                                wp[j * LG * E + 2 * q] = acc[j][q].x;
-                                wp[j * LG * E + 2 * q + 1] = acc[j][q].y;
-                            }
-                        }
-                } else {
-                    TY *yp = Y + (int64_t)cur * ldy + k0 + gl * E;
-#pragma unroll
-                    for (int j = 0; j < NV; j++)
-                        if (kok[j]) {
-                            float a[E];
-#pragma unroll
-                            for (int q = 0; q < E / 2; q++) {
-                                a[2 * q] = acc[j][q].x;
-                                a[2 * q + 1] = acc[j][q].y;
-                            }
-                            store_out<TY, E, VEC_Y>(yp + j * LG * E, a, accumulate != 0);
-                        }
-                }
+        cur++;
+        if (!seg && cur < re) {
+            if (cur - q0 >= 32) {
+                q0 += 32;
+                my_end = q0 + lane < re ? (int32_t)(__ldg(ba.rowptr + q0 + lane + 1) - e_beg) : n_ent;
             }
-#pragma unroll
-            for (int j = 0; j < NV; j++)
-#pragma unroll
-                for (int q = 0; q < E / 2; q++)
-                    acc[j][q] = make_float2(0.f, 0.f);
-            cur++;
-            if (!seg && cur < re) {
-                if (cur - q0 >= 32) {
-                    q0 += 32;
-                    my_end = q0 + lane < re ? (int32_t)(__ldg(ba.rowptr + q0 + lane + 1) - e_beg) : n_ent;
-                }
-                row_end = __shfl_sync(kFull, my_end, cur - q0);
-            }
-        };
-
-        int mc = 0;
-        float mv = 0.f;
-        if (lane < n_ent) {
-            mc = __ldg(colp + lane);
-            mv = __ldg(valp + lane);
+            row_end = __shfl_sync(kFull, my_end, cur - q0);
         }
-        for (int32_t base = 0; base < n_ent; base += 32) {
-            const int n = min(32, n_ent - base);
-            __syncwarp();
-            ent[lane] = make_int2(mc, __float_as_int(mv));
-            __syncwarp();
-            // prefetch the next index batch while this one is consumed
-            if (base + 32 + lane < n_ent) {
-                mc = __ldg(colp + base + 32 + lane);
-                mv = __ldg(valp + base + 32 + lane);
-            }
-            for (int jj = 0; jj < n; jj += R) {
-                raw_t xr[UNROLL][NV];
-                float vv[UNROLL];
-                if (jj + R <= n && base + jj + R <= row_end) {
-                    // the whole round inside the current row: no boundary checks
+    };
+
+    int mc = 0;
+    float mv = 0.f;
+    if (lane < n_ent) {
+        mc = __ldg(colp + lane);
+        mv = __ldg(valp + lane);
+    }
+    for (int32_t base = 0; base < n_ent; base += 32) {
+        const int n = min(32, n_ent - base);
+        __syncwarp();
+        ent[lane] = make_int2(mc, __float_as_int(mv));
+        __syncwarp();
+        // prefetch the next index batch while this one is consumed
+        if (base + 32 + lane < n_ent) {
+            mc = __ldg(colp + base + 32 + lane);
+            mv = __ldg(valp + base + 32 + lane);
+        }
+        for (int jj = 0; jj < n; jj += R) {
+            raw_t xr[UNROLL][NV];
+            float vv[UNROLL];
+            if (jj + R <= n && base + jj + R <= row_end) {
+                // the whole round inside the current row: no boundary checks
 #pragma unroll
-                    for (int u = 0; u < UNROLL; u++) {
-                        const int2 p = ent[jj + u * G + g];
+                for (int u = 0; u < UNROLL; u++) {
+                    const int2 p = ent[jj + u * G + g];
+                    vv[u] = __int_as_float(p.y);
+                    const T *xp = xk + (int64_t)p.x * ldx;
+#pragma unroll
+                    for (int j = 0; j < NV; j++)
+                        if (kok[j])
+                            xr[u][j] = TR::load(xp + j * LG * E);
+                }
+#pragma unroll
+                for (int u = 0; u < UNROLL; u++)
+#pragma unroll
+                    for (int j = 0; j < NV; j++)
+                        fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
+            } else {
+#pragma unroll
+                for (int u = 0; u < UNROLL; u++) {
+                    const int idx = jj + u * G + g;
+                    if (idx < n) {
+                        const int2 p = ent[idx];
                         vv[u] = __int_as_float(p.y);
                         const T *xp = xk + (int64_t)p.x * ldx;
 #pragma unroll
@@ -389,51 +402,50 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
                             if (kok[j])
                                 xr[u][j] = TR::load(xp + j * LG * E);
                     }
-#pragma unroll
-                    for (int u = 0; u < UNROLL; u++)
-#pragma unroll
-                        for (int j = 0; j < NV; j++)
-                            fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
-                } else {
+                }
+                // cut the round [lo, hi) at the row ends it contains
+                int32_t lo = base + jj;
+                const int32_t hi = base + jj + min(R, n - jj);
+                while (true) {
+                    while (lo >= row_end)
+                        flush();
+                    const int32_t sh = min(row_end, hi);
 #pragma unroll
                     for (int u = 0; u < UNROLL; u++) {
-                        const int idx = jj + u * G + g;
-                        if (idx < n) {
-                            const int2 p = ent[idx];
-                            vv[u] = __int_as_float(p.y);
-                            const T *xp = xk + (int64_t)p.x * ldx;
+                        const int32_t e = base + jj + u * G + g;
+                        if (e >= lo && e < sh) {
 #pragma unroll
                             for (int j = 0; j < NV; j++)
-                                if (kok[j])
-                                    xr[u][j] = TR::load(xp + j * LG * E);
+                                fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
                         }
                     }
-                    // cut the round [lo, hi) at the row ends it contains
-                    int32_t lo = base + jj;
-                    const int32_t hi = base + jj + min(R, n - jj);
-                    while (true) {
-                        while (lo >= row_end)
-                            flush();
-                        const int32_t sh = min(row_end, hi);
-#pragma unroll
-                        for (int u = 0; u < UNROLL; u++) {
-                            const int32_t e = base + jj + u * G + g;
-                            if (e >= lo && e < sh) {
-#pragma unroll
-                                for (int j = 0; j < NV; j++)
-                                    fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
-                            }
-                        }
-                        lo = sh;
-                        if (lo >= hi)
-                            break;
-                    }
+                    lo = sh;
+                    if (lo >= hi)
+                        break;
                 }
             }
         }
-        while (cur < re)
-            flush();
     }
+    while (cur < re)
+        flush();
+}
+
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, int MINB = 1>
+__global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __grid_constant__ BlockArgs ba,
+                                                                       const typename ElemOf<TR>::T *__restrict__ X,
+                                                                       int64_t ldx, TY *__restrict__ Y, int64_t ldy,
+                                                                       int K, int accumulate)
+{
+    // the current batch of 32 (col, val) pairs of each warp, read back with
+    // one 8-byte shared-memory load per entry and lane group
+    __shared__ int2 s_ent[kWarpsPerBlock][32];
+    int2 *ent = s_ent[threadIdx.x >> 5];
+    constexpr int W = LG * NV * TR::E;
+    const int k0 = blockIdx.y * W;
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    const int64_t total = ba.nseg + ba.ntask;
+    for (int64_t it = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); it < total; it += nwarps)
+        rowblock_item<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, it, X, ldx, Y, ldy, K, accumulate, k0, ent);
 }
 
 // Hub rows: sum the segment partials ws[s0 .. s1) pairwise — a binary tree in
@@ -474,6 +486,62 @@ __global__ void __launch_bounds__(kThreads) hub_combine_kernel(const int32_t *__
 // i is added to the running block sums of sizes 1, 2, 4, ... that its index's
 // trailing one bits close, so the sum is the same fixed binary tree for every
 // run.  The stack has one slot per tree level (at most 32).
+// One (hub, 128-feature tile) of the combine: partials ws[hub_seg[h] ..
+// hub_seg[h+1]) summed pairwise and written to output row hub_row[h].
+template <typename TY, int UNROLL>
+__device__ __forceinline__ void hub_combine_item(const int32_t *__restrict__ hub_row,
+                                                 const int64_t *__restrict__ hub_seg, const int64_t h, const int tile,
+                                                 const float *__restrict__ ws, const int64_t ld_ws, TY *__restrict__ Y,
+                                                 const int64_t ldy, const int K, const int accumulate)
+{
+    const int lane = threadIdx.x & 31;
+    const int k = tile * 128 + lane * 4;
+    const bool kok = k < K;
+    const int64_t s0 = __ldg(hub_seg + h), m = __ldg(hub_seg + h + 1) - s0;
+    const float *wp = ws + s0 * ld_ws + k;
+    float4 stk[32];
+    for (int64_t i0 = 0; i0 < m; i0 += UNROLL) {
+        float4 v[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; u++)
+            if (kok && i0 + u < m)
+                v[u] = __ldcg(reinterpret_cast<const float4 *>(wp + (i0 + u) * ld_ws));
+#pragma unroll
+        for (int u = 0; u < UNROLL; u++) {
+            const int64_t i = i0 + u;
+            if (i < m) {
+                float4 c = v[u];
+                int l = 0;
+                while ((i >> l) & 1) {
+                    const float4 a = stk[l];
+                    c = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w + c.w);
+                    l++;
+                }
+                stk[l] = c;
+            }
+        }
+    }
+    // fold the open block sums, larger (earlier) blocks first
+    float4 tot = make_float4(0.f, 0.f, 0.f, 0.f);
+    bool first = true;
+    for (int l = 31; l >= 0; l--)
+        if ((m >> l) & 1) {
+            const float4 a = stk[l];
+            tot = first ? a : make_float4(tot.x + a.x, tot.y + a.y, tot.z + a.z, tot.w + a.w);
+            first = false;
+        }
+    if (kok) {
+        const float r[4] = {tot.x, tot.y, tot.z, tot.w};
+        store_out<TY, 4, true>(Y + (int64_t)__ldg(hub_row + h) * ldy + k, r, accumulate != 0);
+    }
+}
+
+// Hub rows, 16-byte vector form (K a multiple of 4, ws rows 16-byte aligned):
+// one warp per (hub, 128-feature tile); every partial is read exactly once,
+// UNROLL partials in flight, and summed pairwise by a binary counter: partial
+// i is added to the running block sums of sizes 1, 2, 4, ... that its index's
+// trailing one bits close, so the sum is the same fixed binary tree for every
+// run.  The stack has one slot per tree level (at most 32).
 template <typename TY, int UNROLL>
 __global__ void __launch_bounds__(kThreads) hub_combine_vec_kernel(const int32_t *__restrict__ hub_row,
                                                                   const int64_t *__restrict__ hub_seg, int64_t nhub,
@@ -481,51 +549,10 @@ __global__ void __launch_bounds__(kThreads) hub_combine_vec_kernel(const int32_t
                                                                   TY *__restrict__ Y, int64_t ldy, int K,
                                                                   int accumulate)
 {
-    const int lane = threadIdx.x & 31;
     const int tiles = (K + 127) / 128;
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
-    for (int64_t w = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); w < nhub * tiles; w += nwarps) {
-        const int64_t h = w / tiles;
-        const int k = (int)(w % tiles) * 128 + lane * 4;
-        const bool kok = k < K;
-        const int64_t s0 = __ldg(hub_seg + h), m = __ldg(hub_seg + h + 1) - s0;
-        const float *wp = ws + s0 * ld_ws + k;
-        float4 stk[32];
-        for (int64_t i0 = 0; i0 < m; i0 += UNROLL) {
-            float4 v[UNROLL];
-#pragma unroll
-            for (int u = 0; u < UNROLL; u++)
-                if (kok && i0 + u < m)
-                    v[u] = __ldcg(reinterpret_cast<const float4 *>(wp + (i0 + u) * ld_ws));
-#pragma unroll
-            for (int u = 0; u < UNROLL; u++) {
-                const int64_t i = i0 + u;
-                if (i < m) {
-                    float4 c = v[u];
-                    int l = 0;
-                    while ((i >> l) & 1) {
-                        const float4 a = stk[l];
-                        c = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w + c.w);
-                        l++;
-                    }
-                    stk[l] = c;
-                }
-            }
-        }
-        // fold the open block sums, larger (earlier) blocks first
-        float4 tot = make_float4(0.f, 0.f, 0.f, 0.f);
-        bool first = true;
-        for (int l = 31; l >= 0; l--)
-            if ((m >> l) & 1) {
-                const float4 a = stk[l];
-                tot = first ? a : make_float4(tot.x + a.x, tot.y + a.y, tot.z + a.z, tot.w + a.w);
-                first = false;
-            }
-        if (kok) {
-            const float r[4] = {tot.x, tot.y, tot.z, tot.w};
-            store_out<TY, 4, true>(Y + (int64_t)__ldg(hub_row + h) * ldy + k, r, accumulate != 0);
-        }
-    }
+    for (int64_t w = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); w < nhub * tiles; w += nwarps)
+        hub_combine_item<TY, UNROLL>(hub_row, hub_seg, w / tiles, (int)(w % tiles), ws, ld_ws, Y, ldy, K, accumulate);
 }
 
 }  // namespace dev

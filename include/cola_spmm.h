@@ -314,6 +314,55 @@ typedef struct cola_spmm_opts {
 cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype x_dtype, int64_t ldx, void *Y, cola_dtype y_dtype,
                       int64_t ldy, int32_t K, const cola_spmm_opts *opts, cola_stream_t stream);
 
+/* ========================================================================
+ * Batched form: many graphs of uneven size, each with its own X, Y and
+ * feature width, in one persistent launch (plus one for hub rows).
+ * ====================================================================== */
+
+typedef struct cola_batch cola_batch;
+
+/* Upload ngraphs partition sets (each split and given its row view, as
+ * cola_graph_upload does); opts applies to all of them and may be NULL. */
+cola_status cola_batch_create(const cola_partition_set *const *parts, int32_t ngraphs, const cola_upload_opts *opts,
+                              cola_batch **out, cola_stream_t stream);
+cola_status cola_batch_free(cola_batch *b);
+
+/* Bind graph g's dense operands: X[g] (>= N_g rows, ldx[g]), Y[g] (N_g rows,
+ * ldy[g]), width K[g]; every X in x_dtype, every Y in y_dtype.  Sizes the
+ * workspaces and uploads the launch descriptors (synchronises `stream`); call
+ * it again when a pointer changes.  Graphs whose operands are not 16-byte
+ * vectors (K not a multiple of 4 FP32 / 8 BF16, unaligned rows) run through
+ * cola_spmm inside cola_batch_run instead of the batched launch. */
+cola_status cola_batch_bind(cola_batch *b, const void *const *X, const int64_t *ldx, void *const *Y,
+                            const int64_t *ldy, const int32_t *K, cola_dtype x_dtype, cola_dtype y_dtype,
+                            cola_stream_t stream);
+
+/* Y[g] = A_g X[g] (or +=, opts->accumulate) for every bound graph.  Only
+ * kernel launches on `stream`: no allocation, no synchronisation. */
+cola_status cola_batch_run(cola_batch *b, const cola_spmm_opts *opts, cola_stream_t stream);
+
+/* Record cola_batch_run into a CUDA graph kept by the batch (replaced by the
+ * next capture or bind), and launch it. */
+cola_status cola_batch_capture(cola_batch *b, const cola_spmm_opts *opts, cola_stream_t stream);
+cola_status cola_batch_replay(cola_batch *b, cola_stream_t stream);
+
+/* Launch parameters of the batched kernel: loads in flight per lane group (2
+ * or 4) and the persistent grid as a percentage of one full wave. */
+cola_status cola_batch_set_params(cola_batch *b, int32_t unroll, int32_t grid_pct);
+
+/* The project's autotuner for the batched launch: times every candidate
+ * (unroll x grid size) on the bound operands with CUDA events, `reps` runs
+ * each, and keeps the fastest (synchronises `stream`). */
+cola_status cola_batch_autotune(cola_batch *b, int32_t reps, cola_stream_t stream, float *best_ms);
+
+typedef struct cola_batch_info {
+    int32_t ngraphs, batched_graphs;
+    int64_t work_items, hub_items, nnz, device_bytes;
+    int32_t unroll, grid_pct;
+    int64_t last_launches;
+} cola_batch_info;
+cola_status cola_batch_get_info(const cola_batch *b, cola_batch_info *out);
+
 #ifdef __cplusplus
 }
 #endif
