@@ -47,6 +47,10 @@ WORKLOADS = {
                       desc="R-MAT scale 21 (2,097,152 nodes), avg degree 48, D^-1/2 A D^-1/2; X 2,097,152x256 "
                            "FP32; P=8 virtual row partitions (the plain FP32 path of the precision form)"),
 }
+BATCHED_DESC = ("512 R-MAT graphs, node counts log-uniform in [1e3, 2e5] (R-MAT at the next power of two, "
+                "induced on the first N nodes), avg degree uniform in [4, 64], row-normalised FP32 values, K from "
+                "{32, 64, 128} FP32, P=4 partitions each; one persistent launch per step, captured in a CUDA graph, "
+                "launch parameters autotuned")
 METRIC = "SpMM HBM GB/s (algorithmic bytes / step time)"
 
 
@@ -431,13 +435,147 @@ def run_ours(args, w):
     return 0
 
 
+def make_batched(count, seed):
+    """The batched workload: per graph (N, row, col, val, K)."""
+    import cola_b200 as cb
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for i in range(count):
+        n = int(round(float(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))))
+        deg = float(rng.uniform(4, 64))
+        K = int(rng.choice([32, 64, 128]))
+        scale = int(np.ceil(np.log2(n)))
+        # deg*n/2 draws at the next power of two, then the subgraph induced on
+        # the first n nodes (R-MAT puts most edges there)
+        _, row, col, _ = cb.rmat(scale, deg * n / float(1 << scale), seed=seed * 100000 + i,
+                                 values=cb.prep.VALUES_NONE)
+        m = (row < n) & (col < n)
+        row, col = row[m], col[m]
+        d = np.bincount(row, minlength=n).astype(np.float64)
+        d[d == 0] = 1.0
+        val = (1.0 / d[row]).astype(np.float32)
+        out.append((n, row, col, val, K))
+    return out
+
+
+def run_batched(args):
+    import torch
+
+    import cola_b200 as cb
+    from cola_b200.batch import Batch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=dev)
+    t0 = time.time()
+    graphs = make_batched(args.batch_graphs, seed=4)
+    psets = [cb.PartitionSet.from_coo(n, r, c, v, 4) for (n, r, c, v, K) in graphs]
+    b = Batch(psets)
+    del psets
+    Xs, Ys, B = [], [], 0
+    xh = []
+    for i, (n, r, c, v, K) in enumerate(graphs):
+        X = dense_x(n, K, 4000 + i)
+        xh.append(X)
+        Xs.append(torch.from_numpy(X).to(dev))
+        Ys.append(torch.empty((n, K), device=dev))
+        B += alg_bytes(len(r), n, K, 4, 4)
+    nnz = sum(len(g[1]) for g in graphs)
+    nodes = sum(g[0] for g in graphs)
+    t_prep = time.time() - t0
+    b.bind(Xs, Ys)
+    stream = torch.cuda.current_stream()
+    tuned_ms = b.autotune(reps=3)
+    cap = torch.cuda.Stream()
+    b.capture(stream=cap)
+    torch.cuda.synchronize()
+    for _ in range(max(args.warmup, 3)):
+        b.replay(stream)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.replay(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # e2e: per graph pinned X -> device, the captured launch, Y -> pinned host
+    e2e_ms = None
+    if not args.no_e2e:
+        Xp = [torch.from_numpy(x).pin_memory() for x in xh]
+        Yp = [torch.empty(y.shape, dtype=y.dtype).pin_memory() for y in Ys]
+        def e2e_step():
+            for x, hx in zip(Xs, Xp):
+                x.copy_(hx, non_blocking=True)
+            b.replay(stream)
+            for y, hy in zip(Ys, Yp):
+                hy.copy_(y, non_blocking=True)
+        e2e_step()
+        torch.cuda.synchronize()
+        steps = max(1, min(args.steps, 5))
+        e0.record(stream)
+        for _ in range(steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / steps
+    # accuracy on three graphs (the largest, a middle one, the smallest)
+    order = np.argsort([g[0] for g in graphs])
+    errs = []
+    for gi in (order[-1], order[len(order) // 2], order[0]):
+        n, r, c, v, K = graphs[gi]
+        errs.append(fp64_error(n, r, c, v, xh[gi], Ys[gi], dev, samples=1024)[0])
+    info = b.info
+    peak, peak_kind = measured_peak()
+    achieved = B / (ms * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": B * world / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": BATCHED_DESC, "graphs": len(graphs), "nodes": nodes, "nnz": nnz,
+                       "batched_graphs": int(info.batched_graphs), "alg_bytes_per_step": B,
+                       "autotuned": {"unroll": int(info.unroll), "grid_pct": int(info.grid_pct),
+                                     "best_ms": tuned_ms},
+                       "parallelism": "replicas x{}".format(world),
+                       "l2": "inputs larger than L2; no flush", "prep_seconds": round(t_prep, 1)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
+                         "kernel_ms": ms, "frac_of_8TBs": achieved / 8000.0},
+            "e2e": None if e2e_ms is None else {
+                "value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
+                "h2d_bytes_per_step": int(sum(x.numel() * 4 for x in Xs)),
+                "d2h_bytes_per_step": int(sum(y.numel() * 4 for y in Ys)), "ms_per_step": e2e_ms},
+            "accuracy": {"rel_frobenius_vs_fp64_max": max(errs), "graphs_checked": 3, "bound": 1e-5},
+            "gpu_launches": int(info.last_launches) * args.steps, "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="fp32", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="fp32", choices=sorted(WORKLOADS) + ["batched"])
+    ap.add_argument("--batch-graphs", type=int, default=512, help="batched workload: number of graphs")
     ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "buffer", "rows"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
@@ -449,6 +587,11 @@ def main():
     ap.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
     ap.add_argument("--K", type=int, default=None, help="override the feature width (exploration runs)")
     args = ap.parse_args()
+    if args.workload == "batched":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched multi-graph form"}))
+            return 0
+        return run_batched(args)
     w = dict(WORKLOADS[args.workload])
     if args.scale is not None:
         w["scale"] = args.scale
