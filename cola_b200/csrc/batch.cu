@@ -213,7 +213,7 @@ cola_status cola_batch_bind(cola_batch *b, const void *const *X, const int64_t *
         d.Y = Y[i];
         d.ldy = ldy[i];
         d.K = K[i];
-        d.lg = dev::kBatchLG;
+        d.lg = dev::batch_lane_width(K[i], xdt == COLA_FLOAT32 ? 4 : 8);
         d.item0 = b->total_items;
         d.hub0 = b->total_hub;
         d.hub_row = g->hub_row;

@@ -16,7 +16,7 @@ struct BatchGraph {
     void *Y;
     int64_t ldy;
     int32_t K;
-    int32_t lg;    // reserved
+    int32_t lg;    // lanes per row tile (8, 16 or 32): batch_lane_width(K, E)
     int64_t item0; // first work item of this graph in the launch
     int64_t hub0;  // first combine item (hub x 128-feature tile) of this graph
     const int32_t *hub_row;
@@ -24,20 +24,23 @@ struct BatchGraph {
     int64_t nhub;
 };
 
-// Every graph runs with the same lane geometry: 8 lanes cover one 128-byte
-// line of an X row (32 FP32 or 64 BF16 features) and the warp's 4 lane groups
-// take interleaved entries, so one warp load instruction fetches 4 lines.  A
-// task walks its graph's feature tiles one after the other (the index batch is
-// re-read from cache per tile; X bytes per entry do not change), so graphs of
-// any width share the one kernel.
-constexpr int kBatchLG = 8;
+// The lane-group width is a per-graph value read at run time (one kernel
+// instantiation for all graphs): lg = 8, 16 or 32 lanes cover one row tile of
+// lg 16-byte vectors, the warp's 32/lg groups take interleaved entries, and
+// rows wider than one tile are walked tile by tile.
+inline int batch_lane_width(int K, int E)
+{
+    int lg = 8;
+    while (lg < 32 && lg * E < K)
+        lg <<= 1;
+    return lg;
+}
 
 template <typename TR, typename TY, int UNROLL>
 __global__ void __launch_bounds__(kThreads, 4) batch_rowblock_kernel(const BatchGraph *__restrict__ gs, int ng,
                                                                      int64_t total, int accumulate)
 {
     using T = typename ElemOf<TR>::T;
-    constexpr int W = kBatchLG * TR::E;  // features per tile
     __shared__ int2 s_ent[kWarpsPerBlock][32];
     int2 *ent = s_ent[threadIdx.x >> 5];
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
@@ -47,10 +50,11 @@ __global__ void __launch_bounds__(kThreads, 4) batch_rowblock_kernel(const Batch
             gi++;
         const BatchGraph &bg = gs[gi];
         const int64_t li = it - bg.item0;
+        const int W = bg.lg * TR::E;  // features per tile
         for (int k0 = 0; k0 < bg.K; k0 += W)
-            rowblock_item<TR, TY, kBatchLG, 1, UNROLL, true>(bg.ba, li, static_cast<const T *>(bg.X), bg.ldx,
-                                                             static_cast<TY *>(bg.Y), bg.ldy, bg.K, accumulate, k0,
-                                                             ent);
+            rowblock_item<TR, TY, 0, 1, UNROLL, true>(bg.ba, li, static_cast<const T *>(bg.X), bg.ldx,
+                                                      static_cast<TY *>(bg.Y), bg.ldy, bg.K, accumulate, k0, ent,
+                                                      bg.lg);
     }
 }
 

@@ -249,25 +249,28 @@ __device__ __forceinline__ void fma_vec2(float2 (&acc)[TR::E / 2], float v, cons
 // [task_rb, task_re) of ba) or a hub segment (its partial goes to ws row `it`).
 // `it` counts segments first, then tasks.  k0 is the first feature of this
 // call's tile; ent is the warp's 32-entry shared-memory index batch.
+// LG > 0 fixes the lane-group width at compile time; LG == 0 takes it from
+// lg_rt at run time (8, 16 or 32), as the batched form does per graph.
 template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y>
 __device__ __forceinline__ void rowblock_item(const BlockArgs &ba, const int64_t it,
                                               const typename ElemOf<TR>::T *__restrict__ X, const int64_t ldx,
                                               TY *__restrict__ Y, const int64_t ldy, const int K, const int accumulate,
-                                              const int k0, int2 *ent)
+                                              const int k0, int2 *ent, const int lg_rt = 0)
 {
     using T = typename ElemOf<TR>::T;
     using raw_t = typename TR::raw_t;
     constexpr int E = TR::E;
-    constexpr int G = 32 / LG;
-    constexpr int R = G * UNROLL;  // entries per round
-    static_assert(R <= 32, "a round must fit in the 32-entry index batch");
+    static_assert(LG == 0 || (32 / LG) * UNROLL <= 32, "a round must fit in the 32-entry index batch");
+    const int lg = LG > 0 ? LG : lg_rt;
+    const int G = 32 / lg;
+    const int R = G * UNROLL;  // entries per round
     const int lane = threadIdx.x & 31;
-    const int g = lane / LG;
-    const int gl = lane % LG;
+    const int g = lane / lg;
+    const int gl = lane % lg;
     bool kok[NV];
 #pragma unroll
     for (int j = 0; j < NV; j++)
-        kok[j] = (k0 + (gl + j * LG) * E) < K;
+        kok[j] = (k0 + (gl + j * lg) * E) < K;
     const T *xk = X + k0 + gl * E;
 
     const bool seg = it < ba.nseg;
@@ -303,7 +306,7 @@ __device__ __forceinline__ void rowblock_item(const BlockArgs &ba, const int64_t
 
     auto flush = [&]() {
 #pragma unroll
-        for (int off = LG; off < 32; off <<= 1)
+        for (int off = lg; off < 32; off <<= 1)
 #pragma unroll
             for (int j = 0; j < NV; j++)
 #pragma unroll
@@ -319,8 +322,8 @@ __device__ __forceinline__ void rowblock_item(const BlockArgs &ba, const int64_t
                     if (kok[j]) {
 #pragma unroll
                         for (int q = 0; q < E / 2; q++) {
-                            wp[j * LG * E + 2 * q] = acc[j][q].x;
-                            wp[j * LG * E + 2 * q + 1] = acc[j][q].y;
+                            wp[j * lg * E + 2 * q] = acc[j][q].x;
+                            wp[j * lg * E + 2 * q + 1] = acc[j][q].y;
                         }
                     }
             } else {
@@ -334,7 +337,7 @@ __device__ __forceinline__ void rowblock_item(const BlockArgs &ba, const int64_t
                             a[2 * q] = acc[j][q].x;
                             a[2 * q + 1] = acc[j][q].y;
                         }
-                        store_out<TY, E, VEC_Y>(yp + j * LG * E, a, accumulate != 0);
+                        store_out<TY, E, VEC_Y>(yp + j * lg * E, a, accumulate != 0);
                     }
             }
         }
@@ -382,7 +385,7 @@ __device__ __forceinline__ void rowblock_item(const BlockArgs &ba, const int64_t
 #pragma unroll
                     for (int j = 0; j < NV; j++)
                         if (kok[j])
-                            xr[u][j] = TR::load(xp + j * LG * E);
+                            xr[u][j] = TR::load(xp + j * lg * E);
                 }
 #pragma unroll
                 for (int u = 0; u < UNROLL; u++)
@@ -400,7 +403,7 @@ __device__ __forceinline__ void rowblock_item(const BlockArgs &ba, const int64_t
 #pragma unroll
                         for (int j = 0; j < NV; j++)
                             if (kok[j])
-                                xr[u][j] = TR::load(xp + j * LG * E);
+                                xr[u][j] = TR::load(xp + j * lg * E);
                     }
                 }
                 // cut the round [lo, hi) at the row ends it contains
