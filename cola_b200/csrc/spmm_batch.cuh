@@ -52,9 +52,9 @@ __global__ void __launch_bounds__(kThreads, 4) batch_rowblock_kernel(const Batch
         const int64_t li = it - bg.item0;
         const int W = bg.lg * TR::E;  // features per tile
         for (int k0 = 0; k0 < bg.K; k0 += W)
-            rowblock_item<TR, TY, 0, 1, UNROLL, true>(bg.ba, li, static_cast<const T *>(bg.X), bg.ldx,
-                                                      static_cast<TY *>(bg.Y), bg.ldy, bg.K, accumulate, k0, ent,
-                                                      bg.lg);
+            rowblock_items<TR, TY, 0, 1, UNROLL, true, const BlockArgs &>(
+                bg.ba, li, 1, li + 1, static_cast<const T *>(bg.X), bg.ldx, static_cast<TY *>(bg.Y), bg.ldy, bg.K,
+                accumulate, k0, ent, bg.lg);
     }
 }
 

@@ -245,14 +245,19 @@ __device__ __forceinline__ void fma_vec2(float2 (&acc)[TR::E / 2], float v, cons
 // every group just accumulates; otherwise it is cut at the row ends, and at
 // every row end the groups' partial sums are added with __shfl_xor_sync and
 // group 0 writes the row.
-// One work item of the streaming schedule: a row-block task (rows
-// [task_rb, task_re) of ba) or a hub segment (its partial goes to ws row `it`).
-// `it` counts segments first, then tasks.  k0 is the first feature of this
-// call's tile; ent is the warp's 32-entry shared-memory index batch.
+// Work items it0, it0 + stride, ... (< total) of the streaming schedule, each a
+// row-block task (rows [task_rb, task_re) of ba) or a hub segment (its partial
+// goes to ws row `it`); items count segments first, then tasks.  k0 is the
+// first feature of this call's tile; ent is the warp's 32-entry shared-memory
+// index batch.
 // LG > 0 fixes the lane-group width at compile time; LG == 0 takes it from
 // lg_rt at run time (8, 16 or 32), as the batched form does per graph.
-template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y>
-__device__ __forceinline__ void rowblock_item(const BlockArgs &ba, const int64_t it,
+// BARef is `const BlockArgs` (the single-graph kernel: arguments read straight
+// from the kernel's parameter space) or `const BlockArgs &` (the batched form:
+// a descriptor in global memory).
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, typename BARef = const BlockArgs>
+__device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, const int64_t stride,
+                                               const int64_t total,
                                               const typename ElemOf<TR>::T *__restrict__ X, const int64_t ldx,
                                               TY *__restrict__ Y, const int64_t ldy, const int K, const int accumulate,
                                               const int k0, int2 *ent, const int lg_rt = 0)
@@ -273,164 +278,166 @@ __device__ __forceinline__ void rowblock_item(const BlockArgs &ba, const int64_t
         kok[j] = (k0 + (gl + j * lg) * E) < K;
     const T *xk = X + k0 + gl * E;
 
-    const bool seg = it < ba.nseg;
-    int32_t rb, re;
-    int64_t e_beg;
-    int32_t n_ent;  // entries of this item; indices below are relative to e_beg
-    if (seg) {
-        rb = __ldg(ba.seg_row + it);
-        re = rb + 1;
-        e_beg = __ldg(ba.seg_beg + it);
-        n_ent = (int32_t)min((int64_t)ba.seg_len, __ldg(ba.rowptr + rb + 1) - e_beg);
-    } else {
-        const int64_t t = it - ba.nseg;
-        rb = __ldg(ba.task_rb + t);
-        re = __ldg(ba.task_re + t);
-        e_beg = __ldg(ba.rowptr + rb);
-        n_ent = (int32_t)(__ldg(ba.rowptr + re) - e_beg);
-    }
-    const int32_t *colp = ba.col + e_beg;
-    const float *valp = ba.val + e_beg;
-    // ends of rows q0 .. q0+31, relative to e_beg (lane l: row q0 + l)
-    int32_t q0 = rb;
-    int32_t my_end = seg ? n_ent : (rb + lane < re ? (int32_t)(__ldg(ba.rowptr + rb + lane + 1) - e_beg) : n_ent);
-    int32_t cur = rb;
-    int32_t row_end = __shfl_sync(kFull, my_end, 0);
-
-    float2 acc[NV][E / 2];
-#pragma unroll
-    for (int j = 0; j < NV; j++)
-#pragma unroll
-        for (int q = 0; q < E / 2; q++)
-            acc[j][q] = make_float2(0.f, 0.f);
-
-    auto flush = [&]() {
-#pragma unroll
-        for (int off = lg; off < 32; off <<= 1)
-#pragma unroll
-            for (int j = 0; j < NV; j++)
-#pragma unroll
-                for (int q = 0; q < E / 2; q++) {
-                    acc[j][q].x += __shfl_xor_sync(kFull, acc[j][q].x, off);
-                    acc[j][q].y += __shfl_xor_sync(kFull, acc[j][q].y, off);
-                }
-        if (g == 0) {
-            if (seg) {
-                float *wp = ba.ws + it * ba.ld_ws + k0 + gl * E;
-#pragma unroll
-                for (int j = 0; j < NV; j++)
-                    if (kok[j]) {
-#pragma unroll
-                        for (int q = 0; q < E / 2; q++) {
-                            wp[j * lg * E + 2 * q] = acc[j][q].x;
-                            wp[j * lg * E + 2 * q + 1] = acc[j][q].y;
-                        }
-                    }
-            } else {
-                TY *yp = Y + (int64_t)cur * ldy + k0 + gl * E;
-#pragma unroll
-                for (int j = 0; j < NV; j++)
-                    if (kok[j]) {
-                        float a[E];
-#pragma unroll
-                        for (int q = 0; q < E / 2; q++) {
-                            a[2 * q] = acc[j][q].x;
-                            a[2 * q + 1] = acc[j][q].y;
-                        }
-                        store_out<TY, E, VEC_Y>(yp + j * lg * E, a, accumulate != 0);
-                    }
-            }
+    for (int64_t it = it0; it < total; it += stride) {
+        const bool seg = it < ba.nseg;
+        int32_t rb, re;
+        int64_t e_beg;
+        int32_t n_ent;  // entries of this item; indices below are relative to e_beg
+        if (seg) {
+            rb = __ldg(ba.seg_row + it);
+            re = rb + 1;
+            e_beg = __ldg(ba.seg_beg + it);
+            n_ent = (int32_t)min((int64_t)ba.seg_len, __ldg(ba.rowptr + rb + 1) - e_beg);
+        } else {
+            const int64_t t = it - ba.nseg;
+            rb = __ldg(ba.task_rb + t);
+            re = __ldg(ba.task_re + t);
+            e_beg = __ldg(ba.rowptr + rb);
+            n_ent = (int32_t)(__ldg(ba.rowptr + re) - e_beg);
         }
-#pragma unroll
+        const int32_t *colp = ba.col + e_beg;
+        const float *valp = ba.val + e_beg;
+        // ends of rows q0 .. q0+31, relative to e_beg (lane l: row q0 + l)
+        int32_t q0 = rb;
+        int32_t my_end = seg ? n_ent : (rb + lane < re ? (int32_t)(__ldg(ba.rowptr + rb + lane + 1) - e_beg) : n_ent);
+        int32_t cur = rb;
+        int32_t row_end = __shfl_sync(kFull, my_end, 0);
+
+        float2 acc[NV][E / 2];
+    #pragma unroll
         for (int j = 0; j < NV; j++)
-#pragma unroll
+    #pragma unroll
             for (int q = 0; q < E / 2; q++)
                 acc[j][q] = make_float2(0.f, 0.f);
-        cur++;
-        if (!seg && cur < re) {
-            if (cur - q0 >= 32) {
-                q0 += 32;
-                my_end = q0 + lane < re ? (int32_t)(__ldg(ba.rowptr + q0 + lane + 1) - e_beg) : n_ent;
-            }
-            row_end = __shfl_sync(kFull, my_end, cur - q0);
-        }
-    };
 
-    int mc = 0;
-    float mv = 0.f;
-    if (lane < n_ent) {
-        mc = __ldg(colp + lane);
-        mv = __ldg(valp + lane);
-    }
-    for (int32_t base = 0; base < n_ent; base += 32) {
-        const int n = min(32, n_ent - base);
-        __syncwarp();
-        ent[lane] = make_int2(mc, __float_as_int(mv));
-        __syncwarp();
-        // prefetch the next index batch while this one is consumed
-        if (base + 32 + lane < n_ent) {
-            mc = __ldg(colp + base + 32 + lane);
-            mv = __ldg(valp + base + 32 + lane);
-        }
-        for (int jj = 0; jj < n; jj += R) {
-            raw_t xr[UNROLL][NV];
-            float vv[UNROLL];
-            if (jj + R <= n && base + jj + R <= row_end) {
-                // the whole round inside the current row: no boundary checks
-#pragma unroll
-                for (int u = 0; u < UNROLL; u++) {
-                    const int2 p = ent[jj + u * G + g];
-                    vv[u] = __int_as_float(p.y);
-                    const T *xp = xk + (int64_t)p.x * ldx;
-#pragma unroll
+        auto flush = [&]() {
+    #pragma unroll
+            for (int off = lg; off < 32; off <<= 1)
+    #pragma unroll
+                for (int j = 0; j < NV; j++)
+    #pragma unroll
+                    for (int q = 0; q < E / 2; q++) {
+                        acc[j][q].x += __shfl_xor_sync(kFull, acc[j][q].x, off);
+                        acc[j][q].y += __shfl_xor_sync(kFull, acc[j][q].y, off);
+                    }
+            if (g == 0) {
+                if (seg) {
+                    float *wp = ba.ws + it * ba.ld_ws + k0 + gl * E;
+    #pragma unroll
                     for (int j = 0; j < NV; j++)
-                        if (kok[j])
-                            xr[u][j] = TR::load(xp + j * lg * E);
+                        if (kok[j]) {
+    #pragma unroll
+                            for (int q = 0; q < E / 2; q++) {
+                                wp[j * lg * E + 2 * q] = acc[j][q].x;
+                                wp[j * lg * E + 2 * q + 1] = acc[j][q].y;
+                            }
+                        }
+                } else {
+                    TY *yp = Y + (int64_t)cur * ldy + k0 + gl * E;
+    #pragma unroll
+                    for (int j = 0; j < NV; j++)
+                        if (kok[j]) {
+                            float a[E];
+    #pragma unroll
+                            for (int q = 0; q < E / 2; q++) {
+                                a[2 * q] = acc[j][q].x;
+                                a[2 * q + 1] = acc[j][q].y;
+                            }
+                            store_out<TY, E, VEC_Y>(yp + j * lg * E, a, accumulate != 0);
+                        }
                 }
-#pragma unroll
-                for (int u = 0; u < UNROLL; u++)
-#pragma unroll
-                    for (int j = 0; j < NV; j++)
-                        fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
-            } else {
-#pragma unroll
-                for (int u = 0; u < UNROLL; u++) {
-                    const int idx = jj + u * G + g;
-                    if (idx < n) {
-                        const int2 p = ent[idx];
+            }
+    #pragma unroll
+            for (int j = 0; j < NV; j++)
+    #pragma unroll
+                for (int q = 0; q < E / 2; q++)
+                    acc[j][q] = make_float2(0.f, 0.f);
+            cur++;
+            if (!seg && cur < re) {
+                if (cur - q0 >= 32) {
+                    q0 += 32;
+                    my_end = q0 + lane < re ? (int32_t)(__ldg(ba.rowptr + q0 + lane + 1) - e_beg) : n_ent;
+                }
+                row_end = __shfl_sync(kFull, my_end, cur - q0);
+            }
+        };
+
+        int mc = 0;
+        float mv = 0.f;
+        if (lane < n_ent) {
+            mc = __ldg(colp + lane);
+            mv = __ldg(valp + lane);
+        }
+        for (int32_t base = 0; base < n_ent; base += 32) {
+            const int n = min(32, n_ent - base);
+            __syncwarp();
+            ent[lane] = make_int2(mc, __float_as_int(mv));
+            __syncwarp();
+            // prefetch the next index batch while this one is consumed
+            if (base + 32 + lane < n_ent) {
+                mc = __ldg(colp + base + 32 + lane);
+                mv = __ldg(valp + base + 32 + lane);
+            }
+            for (int jj = 0; jj < n; jj += R) {
+                raw_t xr[UNROLL][NV];
+                float vv[UNROLL];
+                if (jj + R <= n && base + jj + R <= row_end) {
+                    // the whole round inside the current row: no boundary checks
+    #pragma unroll
+                    for (int u = 0; u < UNROLL; u++) {
+                        const int2 p = ent[jj + u * G + g];
                         vv[u] = __int_as_float(p.y);
                         const T *xp = xk + (int64_t)p.x * ldx;
-#pragma unroll
+    #pragma unroll
                         for (int j = 0; j < NV; j++)
                             if (kok[j])
                                 xr[u][j] = TR::load(xp + j * lg * E);
                     }
-                }
-                // cut the round [lo, hi) at the row ends it contains
-                int32_t lo = base + jj;
-                const int32_t hi = base + jj + min(R, n - jj);
-                while (true) {
-                    while (lo >= row_end)
-                        flush();
-                    const int32_t sh = min(row_end, hi);
-#pragma unroll
+    #pragma unroll
+                    for (int u = 0; u < UNROLL; u++)
+    #pragma unroll
+                        for (int j = 0; j < NV; j++)
+                            fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
+                } else {
+    #pragma unroll
                     for (int u = 0; u < UNROLL; u++) {
-                        const int32_t e = base + jj + u * G + g;
-                        if (e >= lo && e < sh) {
-#pragma unroll
+                        const int idx = jj + u * G + g;
+                        if (idx < n) {
+                            const int2 p = ent[idx];
+                            vv[u] = __int_as_float(p.y);
+                            const T *xp = xk + (int64_t)p.x * ldx;
+    #pragma unroll
                             for (int j = 0; j < NV; j++)
-                                fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
+                                if (kok[j])
+                                    xr[u][j] = TR::load(xp + j * lg * E);
                         }
                     }
-                    lo = sh;
-                    if (lo >= hi)
-                        break;
+                    // cut the round [lo, hi) at the row ends it contains
+                    int32_t lo = base + jj;
+                    const int32_t hi = base + jj + min(R, n - jj);
+                    while (true) {
+                        while (lo >= row_end)
+                            flush();
+                        const int32_t sh = min(row_end, hi);
+    #pragma unroll
+                        for (int u = 0; u < UNROLL; u++) {
+                            const int32_t e = base + jj + u * G + g;
+                            if (e >= lo && e < sh) {
+    #pragma unroll
+                                for (int j = 0; j < NV; j++)
+                                    fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
+                            }
+                        }
+                        lo = sh;
+                        if (lo >= hi)
+                            break;
+                    }
                 }
             }
         }
+        while (cur < re)
+            flush();
     }
-    while (cur < re)
-        flush();
 }
 
 template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, int MINB = 1>
@@ -447,8 +454,8 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
     const int k0 = blockIdx.y * W;
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
     const int64_t total = ba.nseg + ba.ntask;
-    for (int64_t it = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); it < total; it += nwarps)
-        rowblock_item<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, it, X, ldx, Y, ldy, K, accumulate, k0, ent);
+    rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5),
+                                                  nwarps, total, X, ldx, Y, ldy, K, accumulate, k0, ent);
 }
 
 // Hub rows: sum the segment partials ws[s0 .. s1) pairwise — a binary tree in
