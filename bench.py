@@ -51,6 +51,10 @@ BATCHED_DESC = ("512 R-MAT graphs, node counts log-uniform in [1e3, 2e5] (R-MAT 
                 "induced on the first N nodes), avg degree uniform in [4, 64], row-normalised FP32 values, K from "
                 "{32, 64, 128} FP32, P=4 partitions each; one persistent launch per step, captured in a CUDA graph, "
                 "launch parameters autotuned")
+SERVING_DESC = ("64 resident R-MAT graphs (scale uniform in 12..20, avg degree uniform in [8, 48], D^-1/2 A D^-1/2, "
+                "P=8) registered once; Poisson arrivals, each request picks a graph uniformly, K from {16, 64, 256, "
+                "512}, half BF16 and half FP32 (X and Y), X ~N(0,1) in pinned host memory; admission by a 120 GiB "
+                "device budget, 4 slots, requests grouped by (K, dtype) into one launch")
 METRIC = "SpMM HBM GB/s (algorithmic bytes / step time)"
 
 
@@ -568,13 +572,138 @@ def run_batched(args):
     return 0
 
 
+def run_serving(args):
+    import torch
+
+    import cola_b200 as cb
+    from cola_b200.serving import Server
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=dev)
+    t0 = time.time()
+    rng = np.random.Generator(np.random.Philox(5))
+    srv = Server(memory_budget=120 << 30, slots=4, max_group=16)
+    gn, gnnz = [], []
+    for i in range(args.serve_graphs):
+        scale = int(rng.integers(12, 21))
+        deg = float(rng.uniform(8, 48))
+        n, row, col, val = cb.rmat(scale, deg, seed=5000 + i)
+        ps = cb.PartitionSet.from_coo(n, row, col, val, 8)
+        srv.register(ps)
+        gn.append(n)
+        gnnz.append(len(row))
+        del ps, row, col, val
+    max_n = max(gn)
+    Ks = (16, 64, 256, 512)
+    xin, yout = {}, {}
+    for K in Ks:
+        xf = torch.from_numpy(dense_x(max_n, K, 600 + K)).pin_memory()
+        xin[(K, torch.float32)] = xf
+        xin[(K, torch.bfloat16)] = xf.to(torch.bfloat16).pin_memory()
+        # results are not read back by the benchmark: requests of one (K, dtype)
+        # share an output area (the correctness of every result is a test)
+        yout[(K, torch.float32)] = torch.empty((max_n, K), dtype=torch.float32).pin_memory()
+        yout[(K, torch.bfloat16)] = torch.empty((max_n, K), dtype=torch.bfloat16).pin_memory()
+    t_prep = time.time() - t0
+
+    def draw():
+        g = int(rng.integers(0, len(gn)))
+        K = int(rng.choice(Ks))
+        dt = torch.float32 if rng.random() < 0.5 else torch.bfloat16
+        return g, K, dt
+
+    def submit(g, K, dt):
+        n = gn[g]
+        return srv.submit(g, xin[(K, dt)][:n], out_dtype=dt, Y=yout[(K, dt)][:n])
+
+    def req_bytes(g, K, dt):
+        sz = 4 if dt == torch.float32 else 2
+        return alg_bytes(gnnz[g], gn[g], K, sz, sz)
+
+    # warm-up, then the saturation rate: a burst submitted at once
+    for _ in range(max(args.warmup, 3)):
+        submit(*draw()).wait()
+    burst = [draw() for _ in range(args.serve_burst)]
+    tb = time.perf_counter()
+    reqs = [submit(*d) for d in burst]
+    for r in reqs:
+        r.wait()
+    cap = len(burst) / (time.perf_counter() - tb)
+    # open loop: Poisson arrivals at a fraction of the saturation rate
+    rate = args.serve_load * cap
+    nreq = max(args.serve_min_requests, int(rate * args.serve_seconds))
+    srv.reset_stats()
+    clocks = Clocks(local)
+    clocks.start()
+    plan = [draw() for _ in range(nreq)]
+    gaps = rng.exponential(1.0 / rate, nreq)
+    reqs = []
+    ts = time.perf_counter()
+    t_next = ts
+    for d, gap in zip(plan, gaps):
+        t_next += gap
+        delay = t_next - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        reqs.append(submit(*d))
+    for r in reqs:
+        r.wait()
+    wall = time.perf_counter() - ts
+    clk = clocks.stop()
+    st = srv.stats()
+    B = sum(req_bytes(*d) for d in plan)
+    h2d = sum(gn[g] * K * (4 if dt == torch.float32 else 2) for g, K, dt in plan) / nreq
+    value = B / wall / 1e9
+    if world > 1:
+        t = torch.tensor([value], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        value = float(t.item())
+    peak, peak_kind = measured_peak()
+    line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": nreq,
+            "warmup": max(args.warmup, 3), "ms_per_step": wall * 1e3 / nreq, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 and bf16-storage/f32-accum", "data": "synthetic",
+            "config": {"workload": SERVING_DESC, "graphs": len(gn), "nodes": int(sum(gn)), "nnz": int(sum(gnnz)),
+                       "parallelism": "replicas x{}".format(world), "prep_seconds": round(t_prep, 1)},
+            "serving": {"offered_req_per_s": rate, "saturation_req_per_s": cap, "achieved_req_per_s": st["req_per_s"],
+                        "completed": st["completed"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                        "max_ms": st["max_ms"], "mean_ms": st["mean_ms"], "max_inflight": st["max_inflight"],
+                        "groups_launched": st["groups_launched"], "max_group": st["max_group"],
+                        "peak_device_bytes": st["peak_bytes"], "budget_bytes": st["budget"],
+                        "latency": "submit to result in pinned host memory"},
+            "roofline": {"bound": "hbm", "achieved": value / world, "peak": peak, "unit": "GB/s",
+                         "frac": value / world / peak, "traffic": None,
+                         "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
+                         "note": "served rate, PCIe copies of X and Y included"},
+            "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(h2d)},
+            "gpu_launches": None, "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    srv.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="fp32", choices=sorted(WORKLOADS) + ["batched"])
+    ap.add_argument("--workload", default="fp32", choices=sorted(WORKLOADS) + ["batched", "serving"])
+    ap.add_argument("--serve-graphs", type=int, default=64)
+    ap.add_argument("--serve-burst", type=int, default=64, help="serving: requests of the saturation burst")
+    ap.add_argument("--serve-load", type=float, default=0.7, help="serving: offered rate / saturation rate")
+    ap.add_argument("--serve-seconds", type=float, default=20.0, help="serving: length of the open-loop phase")
+    ap.add_argument("--serve-min-requests", type=int, default=100)
     ap.add_argument("--batch-graphs", type=int, default=512, help="batched workload: number of graphs")
     ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "buffer", "rows"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -587,11 +716,12 @@ def main():
     ap.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
     ap.add_argument("--K", type=int, default=None, help="override the feature width (exploration runs)")
     args = ap.parse_args()
-    if args.workload == "batched":
+    if args.workload in ("batched", "serving"):
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched multi-graph form"}))
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no {} form".format(
+                "batched multi-graph" if args.workload == "batched" else "serving")}))
             return 0
-        return run_batched(args)
+        return run_batched(args) if args.workload == "batched" else run_serving(args)
     w = dict(WORKLOADS[args.workload])
     if args.scale is not None:
         w["scale"] = args.scale

@@ -74,6 +74,18 @@ class BatchInfo(ctypes.Structure):
                 ("nnz", I64), ("device_bytes", I64), ("unroll", I32), ("grid_pct", I32), ("last_launches", I64)]
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("memory_budget", I64), ("slots", I32), ("max_group", I32), ("reserved", I32 * 4)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", I64), ("completed", I64), ("rejected", I64), ("cancelled", I64), ("failed", I64),
+                ("pending", I64), ("inflight", I32), ("max_inflight", I32), ("groups_launched", I32),
+                ("max_group", I32), ("bytes_in_use", I64), ("peak_bytes", I64), ("budget", I64),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("req_per_s", ctypes.c_double)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "cola_status_string": (ctypes.c_char_p, [I32]),
@@ -113,6 +125,14 @@ SIGNATURES = {
     "cola_batch_set_params": (I32, [P, I32, I32]),
     "cola_batch_autotune": (I32, [P, I32, P, P]),
     "cola_batch_get_info": (I32, [P, P]),
+    "cola_server_create": (I32, [P, P]),
+    "cola_server_destroy": (I32, [P]),
+    "cola_server_register": (I32, [P, P, P, P]),
+    "cola_server_submit": (I32, [P, I32, P, I32, I32, P, I32, P]),
+    "cola_server_wait": (I32, [P, ctypes.c_uint64, I32]),
+    "cola_server_cancel": (I32, [P, ctypes.c_uint64]),
+    "cola_server_get_stats": (I32, [P, P]),
+    "cola_server_reset_stats": (I32, [P]),
 }
 
 _lib = None

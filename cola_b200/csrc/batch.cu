@@ -12,6 +12,7 @@
 
 #include "common.h"
 #include "graph.h"
+#include "batch.h"
 #include "spmm_batch.cuh"
 
 using cola::dev::BatchGraph;
@@ -67,23 +68,78 @@ static void batch_release(cola_batch *b)
 }
 
 template <typename TR, typename TY, int UNROLL>
-static cola_status launch_batch_t(const cola_batch *b, int accumulate, cudaStream_t st)
+static cola_status launch_batch_t(const BatchLaunch &L, cudaStream_t st)
 {
     auto fn = dev::batch_rowblock_kernel<TR, TY, UNROLL>;
-    int64_t gx = grid_for((const void *)fn, b->total_items);
-    gx = std::max<int64_t>(1, gx * b->grid_pct / 100);
+    int64_t gx = grid_for((const void *)fn, L.total_items);
+    gx = std::max<int64_t>(1, gx * L.grid_pct / 100);
     t_launches++;
-    fn<<<(unsigned)gx, dev::kThreads, 0, st>>>(b->d_desc, (int)b->h_desc.size(), b->total_items, accumulate);
+    fn<<<(unsigned)gx, dev::kThreads, 0, st>>>(L.desc, L.ngraphs, L.total_items, L.accumulate);
     COLA_CUDA(cudaGetLastError());
     return COLA_SUCCESS;
 }
 
 template <typename TR, typename TY>
-static cola_status launch_batch_u(const cola_batch *b, int accumulate, cudaStream_t st)
+static cola_status launch_batch_u(const BatchLaunch &L, cudaStream_t st)
 {
-    if (b->unroll == 2)
-        return launch_batch_t<TR, TY, 2>(b, accumulate, st);
-    return launch_batch_t<TR, TY, 4>(b, accumulate, st);
+    if (L.unroll == 2)
+        return launch_batch_t<TR, TY, 2>(L, st);
+    return launch_batch_t<TR, TY, 4>(L, st);
+}
+
+cola_status launch_batch(const BatchLaunch &L, cudaStream_t st)
+{
+    using BF = __nv_bfloat16;
+    if (L.total_items > 0) {
+        cola_status s;
+        if (L.xdt == COLA_FLOAT32)
+            s = L.ydt == COLA_FLOAT32 ? launch_batch_u<dev::VecTraits<float>, float>(L, st)
+                                      : launch_batch_u<dev::VecTraits<float>, BF>(L, st);
+        else
+            s = L.ydt == COLA_FLOAT32 ? launch_batch_u<dev::VecTraits<BF>, float>(L, st)
+                                      : launch_batch_u<dev::VecTraits<BF>, BF>(L, st);
+        COLA_TRY(s);
+    }
+    if (L.total_hub > 0) {
+        const int64_t blocks = std::min<int64_t>((L.total_hub + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock,
+                                                 (int64_t)sm_count() * 16);
+        t_launches++;
+        if (L.ydt == COLA_FLOAT32)
+            dev::batch_hub_combine_kernel<float, 4><<<(unsigned)blocks, dev::kThreads, 0, st>>>(
+                L.desc, L.ngraphs, L.total_hub, L.accumulate);
+        else
+            dev::batch_hub_combine_kernel<BF, 4><<<(unsigned)blocks, dev::kThreads, 0, st>>>(
+                L.desc, L.ngraphs, L.total_hub, L.accumulate);
+        COLA_CUDA(cudaGetLastError());
+    }
+    return COLA_SUCCESS;
+}
+
+void fill_batch_graph(BatchGraph &d, const cola_graph *g, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t K,
+                      cola_dtype xdt, float *ws)
+{
+    std::memset(&d, 0, sizeof d);
+    d.ba.rowptr = g->rv_ptr;
+    d.ba.col = g->rv_col;
+    d.ba.val = g->rv_val;
+    d.ba.task_rb = g->task_rb;
+    d.ba.task_re = g->task_re;
+    d.ba.ntask = g->ntask;
+    d.ba.seg_row = g->seg_row;
+    d.ba.seg_beg = g->seg_beg;
+    d.ba.nseg = g->nseg;
+    d.ba.seg_len = g->hub_segment;
+    d.ba.ws = ws;
+    d.ba.ld_ws = K;
+    d.X = X;
+    d.ldx = ldx;
+    d.Y = Y;
+    d.ldy = ldy;
+    d.K = K;
+    d.lg = dev::batch_lane_width(K, xdt == COLA_FLOAT32 ? 4 : 8);
+    d.hub_row = g->hub_row;
+    d.hub_seg = g->hub_seg;
+    d.nhub = g->nhub;
 }
 
 static cola_status batch_run(cola_batch *b, const cola_spmm_opts *opts, cudaStream_t st)
@@ -92,30 +148,18 @@ static cola_status batch_run(cola_batch *b, const cola_spmm_opts *opts, cudaStre
     const int accumulate = opts ? opts->accumulate : 0;
     COLA_REQUIRE(!(accumulate && b->ydt != COLA_FLOAT32), COLA_ERROR_UNSUPPORTED,
                  "cola_batch_run: accumulate needs FP32 outputs");
-    using BF = __nv_bfloat16;
     const int64_t before = t_launches;
-    if (b->total_items > 0) {
-        cola_status s;
-        if (b->xdt == COLA_FLOAT32)
-            s = b->ydt == COLA_FLOAT32 ? launch_batch_u<dev::VecTraits<float>, float>(b, accumulate, st)
-                                       : launch_batch_u<dev::VecTraits<float>, BF>(b, accumulate, st);
-        else
-            s = b->ydt == COLA_FLOAT32 ? launch_batch_u<dev::VecTraits<BF>, float>(b, accumulate, st)
-                                       : launch_batch_u<dev::VecTraits<BF>, BF>(b, accumulate, st);
-        COLA_TRY(s);
-    }
-    if (b->total_hub > 0) {
-        const int64_t blocks = std::min<int64_t>((b->total_hub + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock,
-                                                 (int64_t)sm_count() * 16);
-        t_launches++;
-        if (b->ydt == COLA_FLOAT32)
-            dev::batch_hub_combine_kernel<float, 4><<<(unsigned)blocks, dev::kThreads, 0, st>>>(
-                b->d_desc, (int)b->h_desc.size(), b->total_hub, accumulate);
-        else
-            dev::batch_hub_combine_kernel<BF, 4><<<(unsigned)blocks, dev::kThreads, 0, st>>>(
-                b->d_desc, (int)b->h_desc.size(), b->total_hub, accumulate);
-        COLA_CUDA(cudaGetLastError());
-    }
+    BatchLaunch L;
+    L.desc = b->d_desc;
+    L.ngraphs = (int)b->h_desc.size();
+    L.total_items = b->total_items;
+    L.total_hub = b->total_hub;
+    L.xdt = b->xdt;
+    L.ydt = b->ydt;
+    L.unroll = b->unroll;
+    L.grid_pct = b->grid_pct;
+    L.accumulate = accumulate;
+    COLA_TRY(launch_batch(L, st));
     for (const cola_batch::Solo &s : b->solo) {
         cola_spmm_opts o;
         std::memset(&o, 0, sizeof o);
@@ -195,30 +239,9 @@ cola_status cola_batch_bind(cola_batch *b, const void *const *X, const int64_t *
             continue;
         }
         BatchGraph d;
-        std::memset(&d, 0, sizeof d);
-        d.ba.rowptr = g->rv_ptr;
-        d.ba.col = g->rv_col;
-        d.ba.val = g->rv_val;
-        d.ba.task_rb = g->task_rb;
-        d.ba.task_re = g->task_re;
-        d.ba.ntask = g->ntask;
-        d.ba.seg_row = g->seg_row;
-        d.ba.seg_beg = g->seg_beg;
-        d.ba.nseg = g->nseg;
-        d.ba.seg_len = g->hub_segment;
-        d.ba.ws = g->ws_hub;
-        d.ba.ld_ws = K[i];
-        d.X = X[i];
-        d.ldx = ldx[i];
-        d.Y = Y[i];
-        d.ldy = ldy[i];
-        d.K = K[i];
-        d.lg = dev::batch_lane_width(K[i], xdt == COLA_FLOAT32 ? 4 : 8);
+        fill_batch_graph(d, g, X[i], ldx[i], Y[i], ldy[i], K[i], xdt, g->ws_hub);
         d.item0 = b->total_items;
         d.hub0 = b->total_hub;
-        d.hub_row = g->hub_row;
-        d.hub_seg = g->hub_seg;
-        d.nhub = g->nhub;
         b->total_items += g->nseg + g->ntask;
         b->total_hub += g->nhub * ((K[i] + 127) / 128);
         b->h_desc.push_back(d);

@@ -1,0 +1,508 @@
+// Serving loop: graphs registered once stay resident on the device; requests
+// (host X in, host Y out) are admitted by a device-memory budget, grouped by
+// feature width and dtype into one batched launch across graphs, and run on
+// several streams at once, so requests that arrive while others are on the GPU
+// start as soon as a slot and memory free up (continuous batching).
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "batch.h"
+#include "common.h"
+#include "graph.h"
+
+using cola::dev::BatchGraph;
+
+namespace {
+
+double now_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+enum ReqState { kPending = 0, kRunning = 1, kDone = 2, kCancelled = 3, kFailed = 4 };
+
+struct Request {
+    uint64_t id = 0;
+    int32_t graph = 0;
+    const void *X_host = nullptr;
+    void *Y_host = nullptr;
+    cola_dtype xdt = COLA_FLOAT32, ydt = COLA_FLOAT32;
+    int32_t K = 0;
+    int64_t rows = 0;
+    int64_t bytes = 0;  // device bytes while in flight: X + Y + hub workspace
+    double t_submit = 0, t_done = 0;
+    int state = kPending;
+    cola_status status = COLA_SUCCESS;
+    void *dX = nullptr, *dY = nullptr;
+    float *dws = nullptr;
+};
+
+struct Group;
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    Group *busy = nullptr;
+    BatchGraph *d_desc = nullptr;  // descriptor table (device)
+    BatchGraph *h_desc = nullptr;  // staging (pinned)
+    int cap = 0;
+};
+
+struct Group {
+    std::vector<Request *> reqs;
+    int slot = 0;
+    int64_t bytes = 0;
+    bool completed = false;
+};
+
+}  // namespace
+
+struct cola_server {
+    int device = 0;
+    int64_t budget = 0, used = 0, peak_used = 0, graph_bytes = 0;
+    int32_t max_group = 16;
+    std::vector<cola_graph *> graphs;
+    std::vector<Slot> slots;
+    std::mutex mu;
+    std::condition_variable cv_sched, cv_done;
+    std::deque<Request *> pending;
+    std::unordered_map<uint64_t, Request *> reqs;
+    std::vector<Group *> finished;  // groups whose stream work is complete
+    uint64_t next_id = 1;
+    bool stop = false;
+    std::thread th;
+    // statistics
+    int64_t submitted = 0, completed = 0, rejected = 0, cancelled = 0, failed = 0;
+    int32_t inflight = 0, max_inflight = 0, groups_launched = 0, max_group_seen = 0;
+    std::vector<double> lat_ms;
+    double t_first = 0, t_last = 0, t_window = 0;  // statistics cover requests submitted from t_window on
+};
+
+namespace cola {
+
+static void CUDART_CB group_done_cb(void *arg);
+
+struct HostCbArg {
+    cola_server *s;
+    Group *g;
+};
+
+// Launch one admitted group on its slot: copy every X in, run one batched
+// launch over the group's graphs, copy every Y out, then signal completion.
+static cola_status launch_group(cola_server *S, Group *G)
+{
+    Slot &sl = S->slots[(size_t)G->slot];
+    cudaStream_t st = sl.stream;
+    const int n = (int)G->reqs.size();
+    COLA_REQUIRE(n <= sl.cap, COLA_ERROR_INVALID_ARGUMENT, "server: group of %d exceeds the slot's %d", n, sl.cap);
+    const Request *r0 = G->reqs[0];
+    const size_t xs = r0->xdt == COLA_FLOAT32 ? 4 : 2, ys = r0->ydt == COLA_FLOAT32 ? 4 : 2;
+    int64_t items = 0, hub = 0;
+    for (int i = 0; i < n; i++) {
+        Request *r = G->reqs[(size_t)i];
+        const cola_graph *g = S->graphs[(size_t)r->graph];
+        COLA_CUDA(cudaMallocAsync(&r->dX, (size_t)r->rows * r->K * xs, st));
+        COLA_CUDA(cudaMallocAsync(&r->dY, (size_t)r->rows * r->K * ys, st));
+        if (g->nseg > 0)
+            COLA_CUDA(cudaMallocAsync((void **)&r->dws, (size_t)g->nseg * r->K * sizeof(float), st));
+        COLA_CUDA(cudaMemcpyAsync(r->dX, r->X_host, (size_t)r->rows * r->K * xs, cudaMemcpyHostToDevice, st));
+        BatchGraph &d = sl.h_desc[i];
+        fill_batch_graph(d, g, r->dX, r->K, r->dY, r->K, r->K, r->xdt, r->dws);
+        d.item0 = items;
+        d.hub0 = hub;
+        items += g->nseg + g->ntask;
+        hub += g->nhub * ((r->K + 127) / 128);
+    }
+    COLA_CUDA(cudaMemcpyAsync(sl.d_desc, sl.h_desc, (size_t)n * sizeof(BatchGraph), cudaMemcpyHostToDevice, st));
+    BatchLaunch L;
+    L.desc = sl.d_desc;
+    L.ngraphs = n;
+    L.total_items = items;
+    L.total_hub = hub;
+    L.xdt = r0->xdt;
+    L.ydt = r0->ydt;
+    L.unroll = 4;
+    L.grid_pct = 100;
+    L.accumulate = 0;
+    COLA_TRY(launch_batch(L, st));
+    for (Request *r : G->reqs)
+        COLA_CUDA(cudaMemcpyAsync(r->Y_host, r->dY, (size_t)r->rows * r->K * ys, cudaMemcpyDeviceToHost, st));
+    for (Request *r : G->reqs) {
+        COLA_CUDA(cudaFreeAsync(r->dX, st));
+        COLA_CUDA(cudaFreeAsync(r->dY, st));
+        if (r->dws)
+            COLA_CUDA(cudaFreeAsync(r->dws, st));
+        r->dX = r->dY = nullptr;
+        r->dws = nullptr;
+    }
+    HostCbArg *arg = new HostCbArg{S, G};
+    const cudaError_t e = cudaLaunchHostFunc(st, group_done_cb, arg);
+    if (e != cudaSuccess) {
+        delete arg;
+        return fail(COLA_ERROR_CUDA, "server: cudaLaunchHostFunc: %s", cudaGetErrorString(e));
+    }
+    return COLA_SUCCESS;
+}
+
+// Runs on a CUDA driver thread once the group's stream work is done: no CUDA
+// calls here, only hand the group back to the scheduler.
+static void CUDART_CB group_done_cb(void *p)
+{
+    HostCbArg *a = static_cast<HostCbArg *>(p);
+    const double t = now_s();
+    {
+        std::lock_guard<std::mutex> lk(a->s->mu);
+        for (Request *r : a->g->reqs)
+            r->t_done = t;
+        a->g->completed = true;
+        a->s->finished.push_back(a->g);
+    }
+    a->s->cv_sched.notify_all();
+    delete a;
+}
+
+// Scheduler: retire finished groups (return their memory to the budget, wake
+// waiters), then admit pending requests into free slots.  Admission is FIFO:
+// the oldest pending request opens a group of its (K, dtypes) key, later
+// pending requests with the same key join while the group and the budget have
+// room; a head request that does not fit waits for memory to free up.
+static void scheduler(cola_server *S)
+{
+    cudaSetDevice(S->device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    while (true) {
+        S->cv_sched.wait(lk, [&] {
+            if (!S->finished.empty() || (S->stop && S->inflight == 0))
+                return true;
+            if (S->pending.empty())
+                return false;
+            for (const Slot &sl : S->slots)
+                if (!sl.busy)
+                    return true;
+            return false;
+        });
+        // retire
+        for (Group *G : S->finished) {
+            S->slots[(size_t)G->slot].busy = nullptr;
+            S->used -= G->bytes;
+            S->inflight -= (int32_t)G->reqs.size();
+            for (Request *r : G->reqs) {
+                r->state = kDone;
+                if (r->t_submit >= S->t_window) {
+                    S->completed++;
+                    S->lat_ms.push_back((r->t_done - r->t_submit) * 1e3);
+                    S->t_last = std::max(S->t_last, r->t_done);
+                }
+            }
+            delete G;
+        }
+        if (!S->finished.empty())
+            S->cv_done.notify_all();
+        S->finished.clear();
+        if (S->stop && S->pending.empty() && S->inflight == 0)
+            break;
+        // admit
+        while (!S->pending.empty()) {
+            int slot = -1;
+            for (size_t i = 0; i < S->slots.size(); i++)
+                if (!S->slots[i].busy) {
+                    slot = (int)i;
+                    break;
+                }
+            if (slot < 0)
+                break;
+            Request *head = S->pending.front();
+            if (S->used + head->bytes > S->budget)
+                break;  // wait for memory
+            Group *G = new Group();
+            G->slot = slot;
+            for (auto it = S->pending.begin(); it != S->pending.end() && (int32_t)G->reqs.size() < S->max_group;) {
+                Request *r = *it;
+                if (r->K == head->K && r->xdt == head->xdt && r->ydt == head->ydt &&
+                    S->used + G->bytes + r->bytes <= S->budget) {
+                    G->reqs.push_back(r);
+                    G->bytes += r->bytes;
+                    r->state = kRunning;
+                    it = S->pending.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+            S->used += G->bytes;
+            S->peak_used = std::max(S->peak_used, S->used);
+            S->inflight += (int32_t)G->reqs.size();
+            S->max_inflight = std::max(S->max_inflight, S->inflight);
+            S->max_group_seen = std::max(S->max_group_seen, (int32_t)G->reqs.size());
+            S->groups_launched++;
+            S->slots[(size_t)slot].busy = G;
+            // launch without the lock: a CUDA call that waits on the device
+            // must not block the completion callbacks, which take the lock
+            lk.unlock();
+            const cola_status st = launch_group(S, G);
+            lk.lock();
+            if (st != COLA_SUCCESS) {
+                // the group never reaches its callback: release what it queued
+                // and fail it here
+                cudaStream_t sst = S->slots[(size_t)slot].stream;
+                for (Request *r : G->reqs) {
+                    if (r->dX)
+                        cudaFreeAsync(r->dX, sst);
+                    if (r->dY)
+                        cudaFreeAsync(r->dY, sst);
+                    if (r->dws)
+                        cudaFreeAsync(r->dws, sst);
+                    r->dX = r->dY = nullptr;
+                    r->dws = nullptr;
+                }
+                S->slots[(size_t)slot].busy = nullptr;
+                S->used -= G->bytes;
+                S->inflight -= (int32_t)G->reqs.size();
+                for (Request *r : G->reqs) {
+                    r->state = kFailed;
+                    r->status = st;
+                    S->failed++;
+                }
+                delete G;
+                S->cv_done.notify_all();
+            }
+        }
+    }
+}
+
+}  // namespace cola
+
+using namespace cola;
+
+extern "C" {
+
+cola_status cola_server_create(const cola_server_opts *opts, cola_server **out)
+{
+    COLA_REQUIRE(out, COLA_ERROR_INVALID_ARGUMENT, "cola_server_create: out is NULL");
+    *out = nullptr;
+    std::unique_ptr<cola_server> S(new (std::nothrow) cola_server());
+    COLA_REQUIRE(S, COLA_ERROR_OUT_OF_MEMORY, "cola_server_create: host allocation failed");
+    COLA_CUDA(cudaGetDevice(&S->device));
+    S->budget = opts && opts->memory_budget > 0 ? opts->memory_budget : (int64_t)120 << 30;
+    const int nslots = opts && opts->slots > 0 ? opts->slots : 4;
+    S->max_group = opts && opts->max_group > 0 ? opts->max_group : 16;
+    S->slots.resize((size_t)nslots);
+    for (Slot &sl : S->slots) {
+        COLA_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+        COLA_CUDA(cudaMalloc(&sl.d_desc, (size_t)S->max_group * sizeof(BatchGraph)));
+        COLA_CUDA(cudaMallocHost(&sl.h_desc, (size_t)S->max_group * sizeof(BatchGraph)));
+        sl.cap = S->max_group;
+    }
+    S->th = std::thread(scheduler, S.get());
+    *out = S.release();
+    return COLA_SUCCESS;
+}
+
+cola_status cola_server_destroy(cola_server *S)
+{
+    if (!S)
+        return COLA_SUCCESS;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        for (Request *r : S->pending) {  // never admitted: cancel
+            r->state = kCancelled;
+            r->status = COLA_ERROR_CANCELLED;
+        }
+        S->pending.clear();
+    }
+    S->cv_sched.notify_all();
+    S->th.join();  // returns once every admitted group has completed
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(S->device);
+    for (Slot &sl : S->slots) {
+        cudaStreamSynchronize(sl.stream);
+        cudaStreamDestroy(sl.stream);
+        cudaFree(sl.d_desc);
+        cudaFreeHost(sl.h_desc);
+    }
+    for (cola_graph *g : S->graphs)
+        graph_release(g);
+    for (auto &kv : S->reqs)
+        delete kv.second;
+    cudaSetDevice(cur);
+    delete S;
+    return COLA_SUCCESS;
+}
+
+cola_status cola_server_register(cola_server *S, const cola_partition_set *parts, const cola_upload_opts *opts,
+                                 int32_t *graph_id)
+{
+    COLA_REQUIRE(S && parts && graph_id, COLA_ERROR_INVALID_ARGUMENT, "cola_server_register: null argument");
+    COLA_REQUIRE(!(opts && opts->no_row_view), COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_server_register: the server runs on the row view");
+    int cur = 0;
+    COLA_CUDA(cudaGetDevice(&cur));
+    COLA_REQUIRE(cur == S->device, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_server_register: server lives on device %d, current device is %d", S->device, cur);
+    cola_graph *g = nullptr;
+    COLA_TRY(graph_upload(parts, opts, g, nullptr));
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->used + (int64_t)g->dbytes > S->budget) {
+        graph_release(g);
+        return fail(COLA_ERROR_BUDGET, "cola_server_register: graph needs %zu bytes, %lld of %lld bytes in use",
+                    g->dbytes, (long long)S->used, (long long)S->budget);
+    }
+    S->used += (int64_t)g->dbytes;
+    S->graph_bytes += (int64_t)g->dbytes;
+    S->peak_used = std::max(S->peak_used, S->used);
+    S->graphs.push_back(g);
+    *graph_id = (int32_t)S->graphs.size() - 1;
+    return COLA_SUCCESS;
+}
+
+cola_status cola_server_submit(cola_server *S, int32_t graph_id, const void *X_host, cola_dtype x_dtype,
+                               int32_t K, void *Y_host, cola_dtype y_dtype, uint64_t *request_id)
+{
+    COLA_REQUIRE(S && request_id, COLA_ERROR_INVALID_ARGUMENT, "cola_server_submit: null argument");
+    COLA_REQUIRE((x_dtype == COLA_FLOAT32 || x_dtype == COLA_BFLOAT16) &&
+                     (y_dtype == COLA_FLOAT32 || y_dtype == COLA_BFLOAT16),
+                 COLA_ERROR_INVALID_ARGUMENT, "cola_server_submit: unknown dtype");
+    const int E = x_dtype == COLA_FLOAT32 ? 4 : 8;
+    COLA_REQUIRE(K >= 1 && K % E == 0, COLA_ERROR_UNSUPPORTED,
+                 "cola_server_submit: K=%d must be a multiple of %d for this dtype", K, E);
+    std::unique_ptr<Request> r(new (std::nothrow) Request());
+    COLA_REQUIRE(r, COLA_ERROR_OUT_OF_MEMORY, "cola_server_submit: host allocation failed");
+    std::lock_guard<std::mutex> lk(S->mu);
+    COLA_REQUIRE(!S->stop, COLA_ERROR_CANCELLED, "cola_server_submit: server is shutting down");
+    COLA_REQUIRE(graph_id >= 0 && graph_id < (int32_t)S->graphs.size(), COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_server_submit: unknown graph %d", graph_id);
+    const cola_graph *g = S->graphs[(size_t)graph_id];
+    COLA_REQUIRE(g->N == 0 || (X_host && Y_host), COLA_ERROR_INVALID_ARGUMENT, "cola_server_submit: null X or Y");
+    r->graph = graph_id;
+    r->X_host = X_host;
+    r->Y_host = Y_host;
+    r->xdt = x_dtype;
+    r->ydt = y_dtype;
+    r->K = K;
+    r->rows = g->N;
+    r->bytes = (int64_t)g->N * K * ((x_dtype == COLA_FLOAT32 ? 4 : 2) + (y_dtype == COLA_FLOAT32 ? 4 : 2)) +
+               g->nseg * K * 4;
+    if (S->graph_bytes + r->bytes > S->budget) {
+        S->rejected++;
+        return fail(COLA_ERROR_BUDGET,
+                    "cola_server_submit: the request needs %lld device bytes; the budget leaves %lld beside the "
+                    "registered graphs",
+                    (long long)r->bytes, (long long)(S->budget - S->graph_bytes));
+    }
+    r->id = S->next_id++;
+    r->t_submit = now_s();
+    if (S->submitted == 0)
+        S->t_first = r->t_submit;
+    S->submitted++;
+    *request_id = r->id;
+    Request *raw = r.release();
+    S->pending.push_back(raw);
+    S->reqs[raw->id] = raw;
+    S->cv_sched.notify_all();
+    return COLA_SUCCESS;
+}
+
+cola_status cola_server_wait(cola_server *S, uint64_t request_id, int32_t timeout_ms)
+{
+    COLA_REQUIRE(S, COLA_ERROR_INVALID_ARGUMENT, "cola_server_wait: server is NULL");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(request_id);
+    COLA_REQUIRE(it != S->reqs.end(), COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_server_wait: unknown request %llu (or already collected)", (unsigned long long)request_id);
+    Request *r = it->second;
+    auto finished = [&] { return r->state >= kDone; };
+    if (timeout_ms < 0)
+        S->cv_done.wait(lk, finished);
+    else if (!S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), finished))
+        return fail(COLA_ERROR_TIMEOUT, "cola_server_wait: request %llu not finished after %d ms",
+                    (unsigned long long)request_id, timeout_ms);
+    const cola_status st = r->state == kDone ? COLA_SUCCESS : r->status;
+    S->reqs.erase(it);
+    delete r;
+    if (st != COLA_SUCCESS)
+        return fail(st, "cola_server_wait: request %llu %s", (unsigned long long)request_id,
+                    st == COLA_ERROR_CANCELLED ? "was cancelled" : "failed");
+    return COLA_SUCCESS;
+}
+
+cola_status cola_server_cancel(cola_server *S, uint64_t request_id)
+{
+    COLA_REQUIRE(S, COLA_ERROR_INVALID_ARGUMENT, "cola_server_cancel: server is NULL");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(request_id);
+    COLA_REQUIRE(it != S->reqs.end(), COLA_ERROR_INVALID_ARGUMENT, "cola_server_cancel: unknown request %llu",
+                 (unsigned long long)request_id);
+    Request *r = it->second;
+    COLA_REQUIRE(r->state == kPending, COLA_ERROR_NOT_READY,
+                 "cola_server_cancel: request %llu is already on the GPU or finished", (unsigned long long)request_id);
+    S->pending.erase(std::find(S->pending.begin(), S->pending.end(), r));
+    r->state = kCancelled;
+    r->status = COLA_ERROR_CANCELLED;
+    S->cancelled++;
+    S->cv_done.notify_all();
+    return COLA_SUCCESS;
+}
+
+cola_status cola_server_reset_stats(cola_server *S)
+{
+    COLA_REQUIRE(S, COLA_ERROR_INVALID_ARGUMENT, "cola_server_reset_stats: server is NULL");
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->submitted = S->completed = S->rejected = S->cancelled = S->failed = 0;
+    S->max_inflight = S->inflight;
+    S->groups_launched = S->max_group_seen = 0;
+    S->peak_used = S->used;
+    S->lat_ms.clear();
+    S->t_first = S->t_last = 0;
+    S->t_window = now_s();
+    return COLA_SUCCESS;
+}
+
+cola_status cola_server_get_stats(cola_server *S, cola_server_stats *o)
+{
+    COLA_REQUIRE(S && o, COLA_ERROR_INVALID_ARGUMENT, "cola_server_get_stats: null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    std::memset(o, 0, sizeof *o);
+    o->submitted = S->submitted;
+    o->completed = S->completed;
+    o->rejected = S->rejected;
+    o->cancelled = S->cancelled;
+    o->failed = S->failed;
+    o->pending = (int64_t)S->pending.size();
+    o->inflight = S->inflight;
+    o->max_inflight = S->max_inflight;
+    o->groups_launched = S->groups_launched;
+    o->max_group = S->max_group_seen;
+    o->bytes_in_use = S->used;
+    o->peak_bytes = S->peak_used;
+    o->budget = S->budget;
+    if (!S->lat_ms.empty()) {
+        std::vector<double> v = S->lat_ms;
+        std::sort(v.begin(), v.end());
+        auto pct = [&](double q) {
+            return v[(size_t)std::min<double>((double)v.size() - 1, q * (double)(v.size() - 1) + 0.5)];
+        };
+        o->p50_ms = pct(0.50);
+        o->p99_ms = pct(0.99);
+        o->max_ms = v.back();
+        double sum = 0;
+        for (double x : v)
+            sum += x;
+        o->mean_ms = sum / (double)v.size();
+        if (S->t_last > S->t_first)
+            o->req_per_s = (double)S->completed / (S->t_last - S->t_first);
+    }
+    return COLA_SUCCESS;
+}
+
+}  // extern "C"

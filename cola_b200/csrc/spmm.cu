@@ -65,13 +65,6 @@ int64_t grid_for(const void *fn, int64_t items)
 }
 
 
-static int next_pow2(int v)
-{
-    int p = 1;
-    while (p < v)
-        p <<= 1;
-    return p;
-}
 
 // ---------------------------------------------------------------------------
 // fused kernel dispatch
@@ -1062,7 +1055,6 @@ static cola_status spmm_impl(cola_graph *g, const void *X, cola_dtype xdt, int64
         a.accumulate = accumulate;
         a.unroll = opts ? opts->unroll : 0;
         a.min_blocks = opts ? opts->min_blocks : 0;
-        const int V = a.vec ? K / (xdt == COLA_FLOAT32 ? 4 : 8) : 0;
         if (a.vec) {
             dev::BlockArgs ba;
             ba.rowptr = g->rv_ptr;

@@ -265,7 +265,7 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
     using T = typename ElemOf<TR>::T;
     using raw_t = typename TR::raw_t;
     constexpr int E = TR::E;
-    static_assert(LG == 0 || (32 / LG) * UNROLL <= 32, "a round must fit in the 32-entry index batch");
+    static_assert(LG == 0 || (32 / (LG > 0 ? LG : 1)) * UNROLL <= 32, "a round must fit in the 32-entry index batch");
     const int lg = LG > 0 ? LG : lg_rt;
     const int G = 32 / lg;
     const int R = G * UNROLL;  // entries per round

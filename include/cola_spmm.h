@@ -363,6 +363,63 @@ typedef struct cola_batch_info {
 } cola_batch_info;
 cola_status cola_batch_get_info(const cola_batch *b, cola_batch_info *out);
 
+/* ========================================================================
+ * Serving loop: resident graphs, requests admitted by a device-memory
+ * budget, grouped by feature width and dtype into one batched launch across
+ * graphs, several groups in flight on separate streams.
+ * ====================================================================== */
+
+typedef struct cola_server cola_server;
+
+typedef struct cola_server_opts {
+    int64_t memory_budget;  /* device bytes for registered graphs + in-flight requests; 0 = 120 GiB */
+    int32_t slots;          /* groups in flight at once (one CUDA stream each); 0 = 4 */
+    int32_t max_group;      /* requests of one (K, dtypes) launched together; 0 = 16 */
+    int32_t reserved[4];
+} cola_server_opts;
+
+/* Create a server on the current device (opts may be NULL).  A scheduler
+ * thread admits requests as slots and memory free up. */
+cola_status cola_server_create(const cola_server_opts *opts, cola_server **out);
+/* Cancel what is still pending, wait for what is on the GPU, free everything. */
+cola_status cola_server_destroy(cola_server *s);
+
+/* Upload a partition set (split + row view) and keep it resident; its device
+ * bytes count against the budget (COLA_ERROR_BUDGET if they do not fit). */
+cola_status cola_server_register(cola_server *s, const cola_partition_set *parts, const cola_upload_opts *opts,
+                                 int32_t *graph_id);
+
+/* Queue Y = A_graph X.  X_host: N x K row-major host memory in x_dtype (pinned
+ * memory lets the copies overlap); Y_host: N x K in y_dtype, written when the
+ * request completes.  Both must stay valid until cola_server_wait returns.
+ * K must be a multiple of 4 (FP32 X) or 8 (BF16 X).  Returns at once with the
+ * request id; COLA_ERROR_BUDGET if the request could never fit the budget
+ * beside the registered graphs. */
+cola_status cola_server_submit(cola_server *s, int32_t graph_id, const void *X_host, cola_dtype x_dtype, int32_t K,
+                               void *Y_host, cola_dtype y_dtype, uint64_t *request_id);
+
+/* Wait for a request (timeout_ms < 0: no limit).  COLA_SUCCESS: Y_host holds
+ * the result; COLA_ERROR_TIMEOUT: still pending or running (call again);
+ * COLA_ERROR_CANCELLED / other: the request did not run.  A finished request
+ * is forgotten after its wait returns. */
+cola_status cola_server_wait(cola_server *s, uint64_t request_id, int32_t timeout_ms);
+
+/* Cancel a request that has not been admitted yet (COLA_ERROR_NOT_READY if it
+ * is already on the GPU or finished). */
+cola_status cola_server_cancel(cola_server *s, uint64_t request_id);
+
+typedef struct cola_server_stats {
+    int64_t submitted, completed, rejected, cancelled, failed, pending;
+    int32_t inflight, max_inflight, groups_launched, max_group;
+    int64_t bytes_in_use, peak_bytes, budget;
+    double p50_ms, p99_ms, max_ms, mean_ms;  /* submit -> result in host memory */
+    double req_per_s;                        /* completed / (last completion - first submission) */
+} cola_server_stats;
+cola_status cola_server_get_stats(cola_server *s, cola_server_stats *out);
+/* Start a new measurement window: counts, latencies and peaks restart from
+ * the requests submitted after this call (in-flight work is unaffected). */
+cola_status cola_server_reset_stats(cola_server *s);
+
 #ifdef __cplusplus
 }
 #endif
