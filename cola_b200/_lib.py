@@ -75,7 +75,8 @@ class BatchInfo(ctypes.Structure):
 
 
 class ServerOpts(ctypes.Structure):
-    _fields_ = [("memory_budget", I64), ("slots", I32), ("max_group", I32), ("reserved", I32 * 4)]
+    _fields_ = [("memory_budget", I64), ("slots", I32), ("max_group", I32), ("group_mib", I32),
+                ("reserved", I32 * 3)]
 
 
 class ServerStats(ctypes.Structure):
@@ -83,7 +84,9 @@ class ServerStats(ctypes.Structure):
                 ("pending", I64), ("inflight", I32), ("max_inflight", I32), ("groups_launched", I32),
                 ("max_group", I32), ("bytes_in_use", I64), ("peak_bytes", I64), ("budget", I64),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
-                ("mean_ms", ctypes.c_double), ("req_per_s", ctypes.c_double)]
+                ("mean_ms", ctypes.c_double), ("req_per_s", ctypes.c_double), ("queue_ms_mean", ctypes.c_double),
+                ("copy_in_ms_mean", ctypes.c_double), ("kernel_ms_mean", ctypes.c_double),
+                ("copy_out_ms_mean", ctypes.c_double)]
 
 
 # name -> (restype, argtypes)

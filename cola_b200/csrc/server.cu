@@ -41,7 +41,8 @@ struct Request {
     int32_t K = 0;
     int64_t rows = 0;
     int64_t bytes = 0;  // device bytes while in flight: X + Y + hub workspace
-    double t_submit = 0, t_done = 0;
+    int64_t copy_bytes = 0;  // host<->device bytes: X in + Y out
+    double t_submit = 0, t_launch = 0, t_done = 0;
     int state = kPending;
     cola_status status = COLA_SUCCESS;
     void *dX = nullptr, *dY = nullptr;
@@ -56,6 +57,7 @@ struct Slot {
     BatchGraph *d_desc = nullptr;  // descriptor table (device)
     BatchGraph *h_desc = nullptr;  // staging (pinned)
     int cap = 0;
+    cudaEvent_t ev[4] = {};  // group start, X copied in, launch done, Y copied out
 };
 
 struct Group {
@@ -71,8 +73,13 @@ struct cola_server {
     int device = 0;
     int64_t budget = 0, used = 0, peak_used = 0, graph_bytes = 0;
     int32_t max_group = 16;
+    int64_t group_bytes = 32 << 20;
     std::vector<cola_graph *> graphs;
     std::vector<Slot> slots;
+    // request buffers come from a pool of the server's own that keeps freed
+    // memory mapped (release threshold = budget): after warm-up an admitted
+    // request costs no device mapping work
+    cudaMemPool_t pool = nullptr;
     std::mutex mu;
     std::condition_variable cv_sched, cv_done;
     std::deque<Request *> pending;
@@ -85,6 +92,8 @@ struct cola_server {
     int64_t submitted = 0, completed = 0, rejected = 0, cancelled = 0, failed = 0;
     int32_t inflight = 0, max_inflight = 0, groups_launched = 0, max_group_seen = 0;
     std::vector<double> lat_ms;
+    double queue_ms_sum = 0, copy_in_ms_sum = 0, kernel_ms_sum = 0, copy_out_ms_sum = 0;
+    int64_t timed_groups = 0;
     double t_first = 0, t_last = 0, t_window = 0;  // statistics cover requests submitted from t_window on
 };
 
@@ -108,13 +117,14 @@ static cola_status launch_group(cola_server *S, Group *G)
     const Request *r0 = G->reqs[0];
     const size_t xs = r0->xdt == COLA_FLOAT32 ? 4 : 2, ys = r0->ydt == COLA_FLOAT32 ? 4 : 2;
     int64_t items = 0, hub = 0;
+    COLA_CUDA(cudaEventRecord(sl.ev[0], st));
     for (int i = 0; i < n; i++) {
         Request *r = G->reqs[(size_t)i];
         const cola_graph *g = S->graphs[(size_t)r->graph];
-        COLA_CUDA(cudaMallocAsync(&r->dX, (size_t)r->rows * r->K * xs, st));
-        COLA_CUDA(cudaMallocAsync(&r->dY, (size_t)r->rows * r->K * ys, st));
+        COLA_CUDA(cudaMallocFromPoolAsync(&r->dX, (size_t)r->rows * r->K * xs, S->pool, st));
+        COLA_CUDA(cudaMallocFromPoolAsync(&r->dY, (size_t)r->rows * r->K * ys, S->pool, st));
         if (g->nseg > 0)
-            COLA_CUDA(cudaMallocAsync((void **)&r->dws, (size_t)g->nseg * r->K * sizeof(float), st));
+            COLA_CUDA(cudaMallocFromPoolAsync((void **)&r->dws, (size_t)g->nseg * r->K * sizeof(float), S->pool, st));
         COLA_CUDA(cudaMemcpyAsync(r->dX, r->X_host, (size_t)r->rows * r->K * xs, cudaMemcpyHostToDevice, st));
         BatchGraph &d = sl.h_desc[i];
         fill_batch_graph(d, g, r->dX, r->K, r->dY, r->K, r->K, r->xdt, r->dws);
@@ -123,6 +133,7 @@ static cola_status launch_group(cola_server *S, Group *G)
         items += g->nseg + g->ntask;
         hub += g->nhub * ((r->K + 127) / 128);
     }
+    COLA_CUDA(cudaEventRecord(sl.ev[1], st));
     COLA_CUDA(cudaMemcpyAsync(sl.d_desc, sl.h_desc, (size_t)n * sizeof(BatchGraph), cudaMemcpyHostToDevice, st));
     BatchLaunch L;
     L.desc = sl.d_desc;
@@ -135,8 +146,10 @@ static cola_status launch_group(cola_server *S, Group *G)
     L.grid_pct = 100;
     L.accumulate = 0;
     COLA_TRY(launch_batch(L, st));
+    COLA_CUDA(cudaEventRecord(sl.ev[2], st));
     for (Request *r : G->reqs)
         COLA_CUDA(cudaMemcpyAsync(r->Y_host, r->dY, (size_t)r->rows * r->K * ys, cudaMemcpyDeviceToHost, st));
+    COLA_CUDA(cudaEventRecord(sl.ev[3], st));
     for (Request *r : G->reqs) {
         COLA_CUDA(cudaFreeAsync(r->dX, st));
         COLA_CUDA(cudaFreeAsync(r->dY, st));
@@ -174,8 +187,10 @@ static void CUDART_CB group_done_cb(void *p)
 // Scheduler: retire finished groups (return their memory to the budget, wake
 // waiters), then admit pending requests into free slots.  Admission is FIFO:
 // the oldest pending request opens a group of its (K, dtypes) key, later
-// pending requests with the same key join while the group and the budget have
-// room; a head request that does not fit waits for memory to free up.
+// pending requests with the same key join while the group (request count and
+// copy bytes) and the budget have room; a head request that does not fit waits
+// for memory to free up.  The copy-byte cap keeps large requests in groups of
+// their own, so one slot's copy-in overlaps another's launch and copy-out.
 static void scheduler(cola_server *S)
 {
     cudaSetDevice(S->device);
@@ -193,7 +208,20 @@ static void scheduler(cola_server *S)
         });
         // retire
         for (Group *G : S->finished) {
-            S->slots[(size_t)G->slot].busy = nullptr;
+            Slot &sl = S->slots[(size_t)G->slot];
+            if (G->reqs.front()->t_submit >= S->t_window) {
+                float ms[3] = {0, 0, 0};
+                bool ok = true;
+                for (int k = 0; k < 3; k++)
+                    ok = ok && cudaEventElapsedTime(&ms[k], sl.ev[k], sl.ev[k + 1]) == cudaSuccess;
+                if (ok) {
+                    S->copy_in_ms_sum += ms[0];
+                    S->kernel_ms_sum += ms[1];
+                    S->copy_out_ms_sum += ms[2];
+                    S->timed_groups++;
+                }
+            }
+            sl.busy = nullptr;
             S->used -= G->bytes;
             S->inflight -= (int32_t)G->reqs.size();
             for (Request *r : G->reqs) {
@@ -201,6 +229,7 @@ static void scheduler(cola_server *S)
                 if (r->t_submit >= S->t_window) {
                     S->completed++;
                     S->lat_ms.push_back((r->t_done - r->t_submit) * 1e3);
+                    S->queue_ms_sum += (r->t_launch - r->t_submit) * 1e3;
                     S->t_last = std::max(S->t_last, r->t_done);
                 }
             }
@@ -226,12 +255,16 @@ static void scheduler(cola_server *S)
                 break;  // wait for memory
             Group *G = new Group();
             G->slot = slot;
-            for (auto it = S->pending.begin(); it != S->pending.end() && (int32_t)G->reqs.size() < S->max_group;) {
+            int64_t copy = 0;
+            for (auto it = S->pending.begin(); it != S->pending.end() && (int32_t)G->reqs.size() < S->max_group &&
+                                               copy < S->group_bytes;) {
                 Request *r = *it;
                 if (r->K == head->K && r->xdt == head->xdt && r->ydt == head->ydt &&
-                    S->used + G->bytes + r->bytes <= S->budget) {
+                    S->used + G->bytes + r->bytes <= S->budget &&
+                    (G->reqs.empty() || copy + r->copy_bytes <= S->group_bytes)) {
                     G->reqs.push_back(r);
                     G->bytes += r->bytes;
+                    copy += r->copy_bytes;
                     r->state = kRunning;
                     it = S->pending.erase(it);
                 } else {
@@ -245,6 +278,9 @@ static void scheduler(cola_server *S)
             S->max_group_seen = std::max(S->max_group_seen, (int32_t)G->reqs.size());
             S->groups_launched++;
             S->slots[(size_t)slot].busy = G;
+            const double t_launch = now_s();
+            for (Request *r : G->reqs)
+                r->t_launch = t_launch;
             // launch without the lock: a CUDA call that waits on the device
             // must not block the completion callbacks, which take the lock
             lk.unlock();
@@ -295,12 +331,23 @@ cola_status cola_server_create(const cola_server_opts *opts, cola_server **out)
     S->budget = opts && opts->memory_budget > 0 ? opts->memory_budget : (int64_t)120 << 30;
     const int nslots = opts && opts->slots > 0 ? opts->slots : 4;
     S->max_group = opts && opts->max_group > 0 ? opts->max_group : 16;
+    S->group_bytes = (int64_t)(opts && opts->group_mib > 0 ? opts->group_mib : 32) << 20;
+    cudaMemPoolProps pp;
+    std::memset(&pp, 0, sizeof(pp));
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = S->device;
+    COLA_CUDA(cudaMemPoolCreate(&S->pool, &pp));
+    uint64_t keep = (uint64_t)S->budget;
+    COLA_CUDA(cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep));
     S->slots.resize((size_t)nslots);
     for (Slot &sl : S->slots) {
         COLA_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
         COLA_CUDA(cudaMalloc(&sl.d_desc, (size_t)S->max_group * sizeof(BatchGraph)));
         COLA_CUDA(cudaMallocHost(&sl.h_desc, (size_t)S->max_group * sizeof(BatchGraph)));
         sl.cap = S->max_group;
+        for (cudaEvent_t &e : sl.ev)
+            COLA_CUDA(cudaEventCreate(&e));
     }
     S->th = std::thread(scheduler, S.get());
     *out = S.release();
@@ -330,9 +377,14 @@ cola_status cola_server_destroy(cola_server *S)
         cudaStreamDestroy(sl.stream);
         cudaFree(sl.d_desc);
         cudaFreeHost(sl.h_desc);
+        for (cudaEvent_t e : sl.ev)
+            if (e)
+                cudaEventDestroy(e);
     }
     for (cola_graph *g : S->graphs)
         graph_release(g);
+    if (S->pool)
+        cudaMemPoolDestroy(S->pool);
     for (auto &kv : S->reqs)
         delete kv.second;
     cudaSetDevice(cur);
@@ -391,8 +443,8 @@ cola_status cola_server_submit(cola_server *S, int32_t graph_id, const void *X_h
     r->ydt = y_dtype;
     r->K = K;
     r->rows = g->N;
-    r->bytes = (int64_t)g->N * K * ((x_dtype == COLA_FLOAT32 ? 4 : 2) + (y_dtype == COLA_FLOAT32 ? 4 : 2)) +
-               g->nseg * K * 4;
+    r->copy_bytes = (int64_t)g->N * K * ((x_dtype == COLA_FLOAT32 ? 4 : 2) + (y_dtype == COLA_FLOAT32 ? 4 : 2));
+    r->bytes = r->copy_bytes + g->nseg * K * 4;
     if (S->graph_bytes + r->bytes > S->budget) {
         S->rejected++;
         return fail(COLA_ERROR_BUDGET,
@@ -463,6 +515,8 @@ cola_status cola_server_reset_stats(cola_server *S)
     S->groups_launched = S->max_group_seen = 0;
     S->peak_used = S->used;
     S->lat_ms.clear();
+    S->queue_ms_sum = S->copy_in_ms_sum = S->kernel_ms_sum = S->copy_out_ms_sum = 0;
+    S->timed_groups = 0;
     S->t_first = S->t_last = 0;
     S->t_window = now_s();
     return COLA_SUCCESS;
@@ -501,6 +555,12 @@ cola_status cola_server_get_stats(cola_server *S, cola_server_stats *o)
         o->mean_ms = sum / (double)v.size();
         if (S->t_last > S->t_first)
             o->req_per_s = (double)S->completed / (S->t_last - S->t_first);
+        o->queue_ms_mean = S->queue_ms_sum / (double)v.size();
+    }
+    if (S->timed_groups > 0) {
+        o->copy_in_ms_mean = S->copy_in_ms_sum / (double)S->timed_groups;
+        o->kernel_ms_mean = S->kernel_ms_sum / (double)S->timed_groups;
+        o->copy_out_ms_mean = S->copy_out_ms_sum / (double)S->timed_groups;
     }
     return COLA_SUCCESS;
 }

@@ -34,11 +34,12 @@ class Request:
 
 
 class Server:
-    def __init__(self, memory_budget=0, slots=0, max_group=0):
+    def __init__(self, memory_budget=0, slots=0, max_group=0, group_mib=0):
         o = ServerOpts()
         o.memory_budget = int(memory_budget)
         o.slots = int(slots)
         o.max_group = int(max_group)
+        o.group_mib = int(group_mib)
         h = ctypes.c_void_p()
         check(lib().cola_server_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h

@@ -375,7 +375,10 @@ typedef struct cola_server_opts {
     int64_t memory_budget;  /* device bytes for registered graphs + in-flight requests; 0 = 120 GiB */
     int32_t slots;          /* groups in flight at once (one CUDA stream each); 0 = 4 */
     int32_t max_group;      /* requests of one (K, dtypes) launched together; 0 = 16 */
-    int32_t reserved[4];
+    int32_t group_mib;      /* host<->device MiB (X in + Y out) past which a group takes no more
+                               requests, so large requests pipeline copies against other groups'
+                               launches instead of waiting for one long copy phase; 0 = 32 */
+    int32_t reserved[3];
 } cola_server_opts;
 
 /* Create a server on the current device (opts may be NULL).  A scheduler
@@ -414,6 +417,9 @@ typedef struct cola_server_stats {
     int64_t bytes_in_use, peak_bytes, budget;
     double p50_ms, p99_ms, max_ms, mean_ms;  /* submit -> result in host memory */
     double req_per_s;                        /* completed / (last completion - first submission) */
+    double queue_ms_mean;                    /* submit -> the group's launch, per request */
+    /* per group, from CUDA events on the slot's stream: */
+    double copy_in_ms_mean, kernel_ms_mean, copy_out_ms_mean;
 } cola_server_stats;
 cola_status cola_server_get_stats(cola_server *s, cola_server_stats *out);
 /* Start a new measurement window: counts, latencies and peaks restart from
