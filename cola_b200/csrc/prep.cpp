@@ -619,6 +619,31 @@ cola_status cola_nnz_split(const int32_t *rowIdx, int64_t nrows, const int32_t *
     return COLA_SUCCESS;
 }
 
+// rabbit_module/src/reorder.cpp:283-288: edges relabelled by an old -> new map.
+cola_status cola_relabel_edges(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
+                               const int32_t *mapping, int32_t *out_row, int32_t *out_col)
+{
+    clear_error();
+    COLA_REQUIRE(num_nodes >= 0 && nnz >= 0, COLA_ERROR_INVALID_ARGUMENT, "cola_relabel_edges: bad sizes");
+    if (nnz == 0)
+        return COLA_SUCCESS;
+    COLA_REQUIRE(row && col && mapping && out_row && out_col, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_relabel_edges: null arrays");
+    for (int64_t i = 0; i < nnz; i++) {
+        const int32_t r = row[i], c = col[i];
+        COLA_REQUIRE(r >= 0 && r < num_nodes && c >= 0 && c < num_nodes, COLA_ERROR_INVALID_ARGUMENT,
+                     "cola_relabel_edges: entry %lld (%d, %d) outside %d x %d", (long long)i, r, c, num_nodes,
+                     num_nodes);
+        const int32_t mr = mapping[r], mc = mapping[c];
+        COLA_REQUIRE(mr >= 0 && mr < num_nodes && mc >= 0 && mc < num_nodes, COLA_ERROR_INVALID_ARGUMENT,
+                     "cola_relabel_edges: entry %lld or its relabelled ids outside 0..%d", (long long)i,
+                     num_nodes - 1);
+        out_row[i] = mr;
+        out_col[i] = mc;
+    }
+    return COLA_SUCCESS;
+}
+
 cola_status cola_global_csr(int32_t N, int64_t nnz, const int32_t *row, const int32_t *col, const float *val_in,
                             int32_t *rowPtr, int32_t *colIdx, float *val_out, int64_t *nnz_out)
 {

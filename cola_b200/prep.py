@@ -9,7 +9,12 @@ argument meaning:
 * :func:`nnz_split`     -- include/dist_spmm_ppl_batch.cuh:29-56
 * :func:`stage_tables`  -- src/distSpMM_ppl_batch.cu:101-193
 * :func:`bin2vec`       -- include/dist_spmm_ppl_batch.cuh:7-27
+* :func:`relabel_edges` -- rabbit_module/src/reorder.cpp:283-288 (apply a
+  vertex ordering computed elsewhere)
 plus :class:`PartitionSet` (the partitions in memory) and :func:`rmat`.
+:meth:`PartitionSet.from_coo_device`, :func:`nnz_split_device` and
+:func:`relabel_edges` on CUDA tensors run the same steps on the GPU (torch
+tensors in, identical results out).
 """
 import ctypes
 import os
@@ -50,6 +55,24 @@ class PartitionSet:
         h = ctypes.c_void_p()
         check(lib().cola_partition_build(int(num_nodes), len(row), _p(row), _p(col), _p(vv), int(nparts),
                                          ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_coo_device(cls, num_nodes, row, col, val=None, nparts=1):
+        """from_coo with the COO as CUDA tensors (int32 row/col, float32 val):
+        the partitions are built on the GPU, bit-identical to from_coo."""
+        import torch
+        _dev_i32(row, "row")
+        _dev_i32(col, "col")
+        if row.numel() != col.numel() or (val is not None and val.numel() != row.numel()):
+            raise ValueError("row, col and val differ in length")
+        if val is not None and (not val.is_cuda or val.dtype != torch.float32 or not val.is_contiguous()):
+            raise ValueError("val must be a contiguous float32 CUDA tensor")
+        h = ctypes.c_void_p()
+        st = torch.cuda.current_stream(row.device).cuda_stream
+        check(lib().cola_partition_build_device(int(num_nodes), row.numel(), row.data_ptr(), col.data_ptr(),
+                                                None if val is None else val.data_ptr(), int(nparts), st,
+                                                ctypes.byref(h)))
         return cls(h.value)
 
     @classmethod
@@ -179,6 +202,57 @@ def nnz_split(rowIdx, rowPtr, nnz):
     check(lib().cola_nnz_split(_p(rowIdx), len(rowIdx), _p(rowPtr), int(nnz), _p(target), _p(ptr), n.value,
                                ctypes.byref(n)))
     return target[: n.value].copy(), (ptr.copy() if len(rowIdx) else np.zeros(0, I32))
+
+
+def _dev_i32(t, name):
+    import torch
+    if not t.is_cuda or t.dtype != torch.int32 or not t.is_contiguous():
+        raise ValueError("{} must be a contiguous int32 CUDA tensor".format(name))
+
+
+def nnz_split_device(rowIdx, rowPtr, nnz):
+    """nnz_split on CUDA tensors (computed on the GPU) -> (target, ptr) tensors."""
+    import torch
+    _dev_i32(rowIdx, "rowIdx")
+    _dev_i32(rowPtr, "rowPtr")
+    st = torch.cuda.current_stream(rowIdx.device).cuda_stream
+    n = ctypes.c_int64()
+    nrows = rowIdx.numel()
+    check(lib().cola_nnz_split_device(rowIdx.data_ptr(), nrows, rowPtr.data_ptr(), int(nnz), None, None, 0,
+                                      ctypes.byref(n), st))
+    target = torch.empty(max(n.value, 1), dtype=torch.int32, device=rowIdx.device)
+    ptr = torch.empty(n.value + 1, dtype=torch.int32, device=rowIdx.device)
+    if nrows:
+        check(lib().cola_nnz_split_device(rowIdx.data_ptr(), nrows, rowPtr.data_ptr(), int(nnz), target.data_ptr(),
+                                          ptr.data_ptr(), n.value, ctypes.byref(n), st))
+        return target[: n.value], ptr
+    return target[:0], ptr[:0]
+
+
+def relabel_edges(num_nodes, row, col, mapping):
+    """rabbit_module/src/reorder.cpp:283-288: (mapping[row], mapping[col]) for an
+    old -> new vertex mapping computed elsewhere.  numpy arrays are relabelled
+    on the host, CUDA tensors on the GPU."""
+    if hasattr(row, "is_cuda") and row.is_cuda:
+        import torch
+        _dev_i32(row, "row")
+        _dev_i32(col, "col")
+        _dev_i32(mapping, "mapping")
+        out_r = torch.empty_like(row)
+        out_c = torch.empty_like(col)
+        st = torch.cuda.current_stream(row.device).cuda_stream
+        check(lib().cola_relabel_edges_device(int(num_nodes), row.numel(), row.data_ptr(), col.data_ptr(),
+                                              mapping.data_ptr(), out_r.data_ptr(), out_c.data_ptr(), st))
+        return out_r, out_c
+    row = _i32(row)
+    col = _i32(col)
+    mapping = _i32(mapping)
+    if len(row) != len(col):
+        raise ValueError("row and col differ in length")
+    out_r = np.empty_like(row)
+    out_c = np.empty_like(col)
+    check(lib().cola_relabel_edges(int(num_nodes), len(row), _p(row), _p(col), _p(mapping), _p(out_r), _p(out_c)))
+    return out_r, out_c
 
 
 def stage_tables(me, nranks, group_size, num_nodes, csc_colIdx_zip_r, nchunks_l, wg_lists):

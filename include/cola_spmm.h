@@ -100,6 +100,38 @@ cola_status cola_partition_get(const cola_partition_set *s, int32_t part, cola_p
 cola_status cola_nnz_split(const int32_t *rowIdx, int64_t nrows, const int32_t *rowPtr, int64_t nnz,
                            int32_t *target, int32_t *ptr, int64_t capacity, int64_t *nchunks);
 
+/* ------------------------------------------------------------------------
+ * Preprocessing on the device (same outputs, bit for bit, as the host calls
+ * above).  Inputs are device arrays; the calls run on `stream` and return once
+ * their results are complete.
+ * ---------------------------------------------------------------------- */
+
+/* cola_partition_build with the COO (row, col, optional val) in device memory:
+ * the partitions are built by a radix sort on the device and returned as a
+ * host partition set, identical to what cola_partition_build gives for the
+ * same COO.  Needs about 40 bytes of device memory per entry while it runs. */
+cola_status cola_partition_build_device(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
+                                        const float *val, int32_t nparts, cola_stream_t stream,
+                                        cola_partition_set **out);
+
+/* cola_nnz_split on device arrays (rowIdx: nrows, rowPtr: nrows+1; target and
+ * ptr device arrays of capacity / capacity+1 entries).  target == NULL only
+ * counts (*nchunks). */
+cola_status cola_nnz_split_device(const int32_t *rowIdx, int64_t nrows, const int32_t *rowPtr, int64_t nnz,
+                                  int32_t *target, int32_t *ptr, int64_t capacity, int64_t *nchunks,
+                                  cola_stream_t stream);
+
+/* Vertex relabelling of a COO edge list, as rabbit_module/src/reorder.cpp:
+ * 283-288 applies its old -> new id mapping: out_row[i] = mapping[row[i]],
+ * out_col[i] = mapping[col[i]].  The mapping itself (community ordering) is
+ * computed elsewhere; any permutation of 0..num_nodes-1 is accepted.  Host and
+ * device forms; the outputs may alias the inputs. */
+cola_status cola_relabel_edges(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
+                               const int32_t *mapping, int32_t *out_row, int32_t *out_col);
+cola_status cola_relabel_edges_device(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
+                                      const int32_t *mapping, int32_t *out_row, int32_t *out_col,
+                                      cola_stream_t stream);
+
 /* prep_torch_par.py:93-101 (serialize: global CSR).  rowPtr: num_nodes+1;
  * colIdx/val: capacity nnz (val may be NULL). */
 cola_status cola_global_csr(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,

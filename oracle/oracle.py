@@ -109,6 +109,13 @@ def row_partition(num_nodes, row, col, nparts, r, val=None):
     }
 
 
+def relabel_edges(row, col, mapping):
+    """rabbit_module/src/reorder.cpp:283-288: out_row[i] = mapping[src],
+    out_col[i] = mapping[dst] for the old -> new id mapping."""
+    mapping = np.asarray(mapping)
+    return mapping[np.asarray(row)].astype(np.int32), mapping[np.asarray(col)].astype(np.int32)
+
+
 def global_csr(num_nodes, row, col, val=None):
     """prep_torch_par.py:93-101 (A.tocsr())."""
     L = lib()

@@ -223,3 +223,21 @@ def test_rmat_properties():
     d3 = np.bincount(r3, minlength=1024)
     assert np.all(np.isin(np.arange(1024), r3[r3 == c3]))
     np.testing.assert_allclose(v3, 1.0 / d3[r3], rtol=1e-6)
+
+
+def test_relabel_edges_matches_oracle():
+    n, row, col, _ = cb.rmat(10, 8, seed=5)
+    mapping = np.random.Generator(np.random.Philox(5)).permutation(n).astype(np.int32)
+    r, c = cb.relabel_edges(n, row, col, mapping)
+    wr, wc = oracle.relabel_edges(row, col, mapping)
+    np.testing.assert_array_equal(r, wr)
+    np.testing.assert_array_equal(c, wc)
+
+
+def test_relabel_edges_rejects_bad_ids():
+    row = np.array([0, 1], np.int32)
+    col = np.array([1, 4], np.int32)
+    with pytest.raises(cb.ColaError):
+        cb.relabel_edges(4, row, col, np.arange(4, dtype=np.int32))  # col 4 outside
+    with pytest.raises(cb.ColaError):
+        cb.relabel_edges(4, row, col[:1].repeat(2), np.array([0, 9, 1, 2], np.int32))  # maps to 9
