@@ -56,6 +56,9 @@ SERVING_DESC = ("64 resident R-MAT graphs (scale uniform in 12..20, avg degree u
                 "512}, half BF16 and half FP32 (X and Y), X ~N(0,1) in pinned host memory; admission by a 120 GiB "
                 "device budget, 4 slots, requests grouped by (K, dtype) into one launch")
 METRIC = "SpMM HBM GB/s (algorithmic bytes / step time)"
+PREP_METRIC = "partition build throughput (COO entries / s)"
+PREP_DESC = ("partition build of R-MAT scale 20, avg degree 32 (33.5 M COO entries, D^-1/2 A D^-1/2 values), "
+             "P=8: local CSR + compacted remote CSC per partition, duplicates merged, as prep_torch_par.py:24-79")
 
 
 def alg_bytes(nnz, M, K, s_x, s_y, s_v=4):
@@ -698,13 +701,156 @@ def run_serving(args):
     return 0
 
 
+def prep_case():
+    import cola_b200 as cb
+    return cb.rmat(20, 32, seed=2), 8
+
+
+def oracle_partitions(n, row, col, val, P, nthreads):
+    """The oracle's row_partition for every partition, partitions spread over
+    host threads (the C calls release the GIL).  Returns seconds."""
+    import concurrent.futures as cf
+
+    from oracle import oracle
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=nthreads) as ex:
+        list(ex.map(lambda r: oracle.row_partition(n, row, col, P, r, val), range(P)))
+    return time.perf_counter() - t0
+
+
+def prep_sort_passes(n, P):
+    npp = (n + P - 1) // P
+    bits = (max(npp - 1, 0)).bit_length() + (max(n - 1, 0)).bit_length() + (2 * P - 1).bit_length()
+    return (bits + 7) // 8
+
+
+def run_prep_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    (n, row, col, val), P = prep_case()
+    nth = min(host_threads(), P)
+    for _ in range(max(args.warmup - 1, 0)):
+        oracle_partitions(n, row, col, val, P, nth)
+    times = [oracle_partitions(n, row, col, val, P, nth) for _ in range(args.steps)]
+    t = sum(times) / len(times)
+    v = len(row) / t / 1e6
+    line = {"impl": "reference", "metric": PREP_METRIC, "value": v, "unit": "M entries/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": PREP_DESC, "nnz": len(row), "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": "M entries/s", "cores": nth, "kind": "port",
+                             "sample": "the whole workload: the oracle's row_partition (a C restatement of "
+                                       "prep_torch_par.py:24-79; the reference's own is Python/scipy) for all {} "
+                                       "partitions on {} threads".format(P, nth)},
+            "e2e": {"value": v, "unit": "M entries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_prep(args):
+    import torch
+
+    import cola_b200 as cb
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=dev)
+    (n, row, col, val), P = prep_case()
+    nnz = len(row)
+    rh = torch.from_numpy(row).pin_memory()
+    ch = torch.from_numpy(col).pin_memory()
+    vh = torch.from_numpy(val).pin_memory()
+    rd, cd, vd = rh.to(dev), ch.to(dev), vh.to(dev)
+    stream = torch.cuda.current_stream()
+
+    def build(r, c, v):
+        return cb.PartitionSet.from_coo_device(n, r, c, v, P)
+
+    for _ in range(max(args.warmup, 3)):
+        build(rd, cd, vd).close()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    for _ in range(args.steps):
+        build(rd, cd, vd).close()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # end to end: pinned host COO -> device, build, partitions in host memory
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 5))
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        ps = build(rh.to(dev, non_blocking=True), ch.to(dev, non_blocking=True), vh.to(dev, non_blocking=True))
+        d2h = 0
+        for r in range(P):
+            v = ps.part_view(r)
+            d2h += 4 * (v.n_rowPtr_l + 2 * v.nnz_l + v.n_rows_l + v.n_colPtr_r + 2 * v.nnz_r + v.n_cols_r)
+        ps.close()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    # parity of this very workload against the product's host build
+    ref = cb.PartitionSet.from_coo(n, row, col, val, P)
+    got = build(rd, cd, vd)
+    same = all(np.array_equal(got.part(r)[k], ref.part(r)[k]) for r in range(P) for k in
+               ("csr_rowPtr_l", "csr_colIdx_l", "csr_rowIdx_l", "csc_colPtr_r", "csc_rowIdx_r", "csc_colIdx_r",
+                "csr_val_l", "csc_val_r"))
+    passes = prep_sort_passes(n, P)
+    sort_bytes = 32 * passes * nnz
+    peak, peak_kind = measured_peak()
+    achieved = sort_bytes / (ms * 1e-3) / 1e9
+    line = {"metric": PREP_METRIC, "value": nnz * world / (ms * 1e-3) / 1e6, "unit": "M entries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32 (+ f32 value sums)", "data": "synthetic",
+            "config": {"workload": PREP_DESC, "nnz": nnz, "nparts": P, "radix_passes": passes,
+                       "parallelism": "replicas x{}".format(world),
+                       "l2": "inputs larger than L2 (sort buffers {:.0f} MiB); no flush".format(24 * nnz / 2 ** 20)},
+            "parity": {"identical_to_host_build": bool(same)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
+                         "note": "radix sort bytes (32 B per entry per 8-bit pass) over the whole build's time"},
+            "e2e": {"value": nnz * world / (e2e_ms * 1e-3) / 1e6, "unit": "M entries/s",
+                    "h2d_bytes_per_step": 12 * nnz, "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
+            # per build: range check, keys, 5 per radix pass (counts, 3-launch scan, scatter),
+            # 2 x (scan + pass) for duplicates and rows, group bounds, 3 output launches
+            "gpu_launches": (14 + 5 * passes) * args.steps, "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t = oracle_partitions(n, row, col, val, P, 1)
+        line["cpu_baseline"] = {"value": nnz / t / 1e6, "unit": "M entries/s", "cores": 1, "kind": "port",
+                                "sample": "the whole workload once: the oracle's row_partition (C restatement of "
+                                          "prep_torch_par.py:24-79) for all {} partitions, one thread".format(P)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0 if same else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="fp32", choices=sorted(WORKLOADS) + ["batched", "serving"])
+    ap.add_argument("--workload", default="fp32", choices=sorted(WORKLOADS) + ["batched", "serving", "prep"])
     ap.add_argument("--serve-graphs", type=int, default=64)
     ap.add_argument("--serve-burst", type=int, default=64, help="serving: requests of the saturation burst")
     ap.add_argument("--serve-load", type=float, default=0.7, help="serving: offered rate / saturation rate")
@@ -722,6 +868,8 @@ def main():
     ap.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
     ap.add_argument("--K", type=int, default=None, help="override the feature width (exploration runs)")
     args = ap.parse_args()
+    if args.workload == "prep":
+        return run_prep_reference(args) if args.impl == "reference" else run_prep(args)
     if args.workload in ("batched", "serving"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no {} form".format(

@@ -424,8 +424,8 @@ cola_status partition_write_bin(const cola_partition_set *s, const char *dir)
     return COLA_SUCCESS;
 }
 
-template <typename T>
-static cola_status read_vec(const std::string &path, std::vector<T> &v, bool optional, bool *present)
+template <typename T, typename A>
+static cola_status read_vec(const std::string &path, std::vector<T, A> &v, bool optional, bool *present)
 {
     struct stat st;
     if (stat(path.c_str(), &st) != 0) {

@@ -1,19 +1,49 @@
 // Host-side partition structures and preprocessing steps (see prep.cpp).
 #pragma once
 #include <cstdint>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "cola_spmm.h"
 
 namespace cola {
 
+// Allocator whose resize() leaves new elements uninitialised: partition
+// arrays are always written in full after sizing, so large ones are not
+// zero-filled first.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept
+    {
+    }
+    template <class U>
+    void construct(U *p) noexcept
+    {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U *p, A &&...a)
+    {
+        ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+    }
+};
+using ivec = std::vector<int32_t, NoInitAlloc<int32_t>>;
+using fvec = std::vector<float, NoInitAlloc<float>>;
+
 // One virtual partition as prep_torch_par.py:24-79 writes it, plus values.
 struct PartHost {
     int32_t part = 0, row_lb = 0, row_ub = 0;
-    std::vector<int32_t> l_rowPtr, l_colIdx, l_rowIdx;  // local CSR (col % npp), non-empty rows
-    std::vector<float> l_val;
-    std::vector<int32_t> r_colPtr, r_rowIdx, r_colIdx;  // remote CSC (global cols), non-empty cols
-    std::vector<float> r_val;
+    ivec l_rowPtr, l_colIdx, l_rowIdx;  // local CSR (col % npp), non-empty rows
+    fvec l_val;
+    ivec r_colPtr, r_rowIdx, r_colIdx;  // remote CSC (global cols), non-empty cols
+    fvec r_val;
 };
 
 // Tables of src/distSpMM_ppl_batch.cu:101-193 for one PE.

@@ -21,6 +21,8 @@
 #include <climits>
 #include <cstring>
 #include <memory>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -402,30 +404,131 @@ inline unsigned grid_stride_blocks(int64_t n)
     return (unsigned)(need < 1 ? 1 : need < cap ? need : cap);
 }
 
-// Stream-ordered scratch memory freed on every exit path.
+// Scratch device memory for one call, released on every exit path: carved
+// from one arena when the caller reserves one (a single mapping per call, kept
+// for the whole call), else one stream-ordered allocation per request.
 struct Scratch {
     cudaStream_t st;
     std::vector<void *> ptrs;
+    char *arena = nullptr;
+    size_t used = 0, cap = 0;
     explicit Scratch(cudaStream_t s) : st(s) {}
     ~Scratch()
     {
         for (void *p : ptrs)
             cudaFreeAsync(p, st);
     }
-    template <class T>
-    cola_status get(T *&p, int64_t count)
+    cola_status alloc(void *&q, size_t bytes)
     {
-        void *q = nullptr;
-        const size_t bytes = (size_t)(count > 0 ? count : 1) * sizeof(T);
         const cudaError_t e = cudaMallocAsync(&q, bytes, st);
         if (e != cudaSuccess)
             return fail(e == cudaErrorMemoryAllocation ? COLA_ERROR_OUT_OF_MEMORY : COLA_ERROR_CUDA,
                         "device preprocessing: cudaMallocAsync(%zu): %s", bytes, cudaGetErrorString(e));
         ptrs.push_back(q);
+        return COLA_SUCCESS;
+    }
+    cola_status reserve(size_t bytes)
+    {
+        void *q = nullptr;
+        COLA_TRY(alloc(q, bytes));
+        arena = static_cast<char *>(q);
+        cap = bytes;
+        used = 0;
+        return COLA_SUCCESS;
+    }
+    template <class T>
+    cola_status get(T *&p, int64_t count)
+    {
+        const size_t bytes = ((size_t)(count > 0 ? count : 1) * sizeof(T) + 255) & ~(size_t)255;
+        if (arena && used + bytes <= cap) {
+            p = reinterpret_cast<T *>(arena + used);
+            used += bytes;
+            return COLA_SUCCESS;
+        }
+        void *q = nullptr;
+        COLA_TRY(alloc(q, bytes));
         p = static_cast<T *>(q);
         return COLA_SUCCESS;
     }
 };
+
+// Device -> host copies through a pinned double buffer: chunk i + 1 crosses
+// PCIe while host threads spread chunk i into its destinations, so large
+// results reach pageable host memory near link speed.  One staging area per
+// process, grown on demand, used by one call at a time.
+struct HostCopy {
+    void *dst;
+    const void *src;
+    size_t bytes;
+};
+
+static std::mutex g_stage_mu;
+static char *g_stage[2] = {nullptr, nullptr};
+static cudaEvent_t g_stage_ev[2] = {nullptr, nullptr};
+constexpr size_t kStageBytes = 16u << 20;
+
+static cola_status copy_to_host(const std::vector<HostCopy> &jobs, cudaStream_t st)
+{
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    for (int b = 0; b < 2; b++) {
+        if (!g_stage[b])
+            COLA_CUDA(cudaMallocHost((void **)&g_stage[b], kStageBytes));
+        if (!g_stage_ev[b])
+            COLA_CUDA(cudaEventCreateWithFlags(&g_stage_ev[b], cudaEventDisableTiming));
+    }
+    // pieces of at most one chunk, packed into chunks in order
+    struct Piece {
+        char *dst;
+        const char *src;
+        size_t bytes, off;  // off: position in its chunk
+    };
+    std::vector<std::vector<Piece>> chunks(1);
+    size_t fill = 0;
+    for (const HostCopy &j : jobs) {
+        size_t done = 0;
+        while (done < j.bytes) {
+            if (fill == kStageBytes) {
+                chunks.emplace_back();
+                fill = 0;
+            }
+            const size_t n = std::min(j.bytes - done, kStageBytes - fill);
+            chunks.back().push_back(
+                {static_cast<char *>(j.dst) + done, static_cast<const char *>(j.src) + done, n, fill});
+            fill += n;
+            done += n;
+        }
+    }
+    auto issue = [&](size_t c) -> cola_status {
+        char *buf = g_stage[c & 1];
+        for (const Piece &p : chunks[c])
+            COLA_CUDA(cudaMemcpyAsync(buf + p.off, p.src, p.bytes, cudaMemcpyDeviceToHost, st));
+        COLA_CUDA(cudaEventRecord(g_stage_ev[c & 1], st));
+        return COLA_SUCCESS;
+    };
+    if (chunks[0].empty())
+        return COLA_SUCCESS;
+    COLA_TRY(issue(0));
+    for (size_t c = 0; c < chunks.size(); c++) {
+        if (c + 1 < chunks.size())
+            COLA_TRY(issue(c + 1));  // the other buffer: its previous chunk was spread already
+        COLA_CUDA(cudaEventSynchronize(g_stage_ev[c & 1]));
+        const char *buf = g_stage[c & 1];
+        const std::vector<Piece> &ps = chunks[c];
+        // spread in 256 KiB slices over the host threads
+        constexpr size_t kSlice = 256u << 10;
+        std::vector<std::pair<size_t, size_t>> work;  // (piece, slice start)
+        for (size_t i = 0; i < ps.size(); i++)
+            for (size_t o = 0; o < ps[i].bytes; o += kSlice)
+                work.emplace_back(i, o);
+#pragma omp parallel for schedule(dynamic, 4)
+        for (int64_t w = 0; w < (int64_t)work.size(); w++) {
+            const Piece &p = ps[work[(size_t)w].first];
+            const size_t o = work[(size_t)w].second;
+            std::memcpy(p.dst + o, buf + p.off + o, std::min(kSlice, p.bytes - o));
+        }
+    }
+    return COLA_SUCCESS;
+}
 
 // out[i] = exclusive prefix sum of f(0..i-1) for i < n; *total (host) = sum.
 template <class F>
@@ -508,12 +611,21 @@ static cola_status partition_build_device(int32_t N, int64_t nnz, const int32_t 
         return COLA_SUCCESS;
     }
     Scratch sc(st);
+    const int64_t ntiles = (nnz + kTile - 1) / kTile;
+    {
+        // every buffer below, each rounded to 256 bytes, plus the scans' block sums
+        const size_t n = (size_t)nnz, a = 256;
+        const size_t scan_blocks = (size_t)((std::max<int64_t>(ntiles * kBins, nnz) + kScanTile - 1) / kScanTile) + 1;
+        const size_t bytes = 2 * (8 * n + a) + 2 * (4 * n + a) + (4 * (size_t)ntiles * kBins + a) + 4 * (4 * n + a) +
+                             (4 * (n + (size_t)G) + a) + 2 * (8 * ((size_t)G + 1) + a) + 2 * a +
+                             (2 * 6 + 16) * (4 * scan_blocks + a);
+        COLA_TRY(sc.reserve(bytes));
+    }
     COLA_TRY(check_range(row, col, nnz, N, sc, who));
 
     // sort
     uint64_t *k0 = nullptr, *k1 = nullptr;
     uint32_t *v0 = nullptr, *v1 = nullptr, *hist = nullptr, *d_total = nullptr;
-    const int64_t ntiles = (nnz + kTile - 1) / kTile;
     COLA_TRY(sc.get(k0, nnz));
     COLA_TRY(sc.get(k1, nnz));
     COLA_TRY(sc.get(v0, nnz));
@@ -572,6 +684,7 @@ static cola_status partition_build_device(int32_t N, int64_t nnz, const int32_t 
     COLA_CUDA(cudaMemcpyAsync(hu.data(), u_off, hu.size() * 8, cudaMemcpyDeviceToHost, st));
     COLA_CUDA(cudaMemcpyAsync(hs.data(), s_off, hs.size() * 8, cudaMemcpyDeviceToHost, st));
     COLA_CUDA(cudaStreamSynchronize(st));
+    std::vector<HostCopy> jobs;
     try {
         for (int32_t r = 0; r < nparts; r++) {
             PartHost &P = s->parts[(size_t)r];
@@ -579,30 +692,28 @@ static cola_status partition_build_device(int32_t N, int64_t nnz, const int32_t 
                 const int g = 2 * r + rem;
                 const int64_t u0 = hu[(size_t)g], nu = hu[(size_t)g + 1] - u0;
                 const int64_t s0 = hs[(size_t)g], ns = hs[(size_t)g + 1] - s0;
-                std::vector<int32_t> &ent = rem ? P.r_rowIdx : P.l_colIdx;
-                std::vector<float> &v = rem ? P.r_val : P.l_val;
-                std::vector<int32_t> &ids = rem ? P.r_colIdx : P.l_rowIdx;
-                std::vector<int32_t> &ptrs = rem ? P.r_colPtr : P.l_rowPtr;
+                ivec &ent = rem ? P.r_rowIdx : P.l_colIdx;
+                fvec &v = rem ? P.r_val : P.l_val;
+                ivec &ids = rem ? P.r_colIdx : P.l_rowIdx;
+                ivec &ptrs = rem ? P.r_colPtr : P.l_rowPtr;
                 ent.resize((size_t)nu);
                 v.resize((size_t)nu);
                 ids.resize((size_t)ns);
                 ptrs.resize((size_t)ns + 1);
                 if (nu > 0) {
-                    COLA_CUDA(cudaMemcpyAsync(ent.data(), sec + u0, (size_t)nu * 4, cudaMemcpyDeviceToHost, st));
-                    COLA_CUDA(cudaMemcpyAsync(v.data(), uval + u0, (size_t)nu * 4, cudaMemcpyDeviceToHost, st));
-                    COLA_CUDA(cudaMemcpyAsync(ids.data(), prim + s0, (size_t)ns * 4, cudaMemcpyDeviceToHost, st));
-                    COLA_CUDA(cudaMemcpyAsync(ptrs.data(), ptr + s0 + g, (size_t)(ns + 1) * 4, cudaMemcpyDeviceToHost,
-                                              st));
+                    jobs.push_back({ent.data(), sec + u0, (size_t)nu * 4});
+                    jobs.push_back({v.data(), uval + u0, (size_t)nu * 4});
+                    jobs.push_back({ids.data(), prim + s0, (size_t)ns * 4});
+                    jobs.push_back({ptrs.data(), ptr + s0 + g, (size_t)(ns + 1) * 4});
                 } else {
                     ptrs[0] = 0;
                 }
             }
         }
     } catch (const std::bad_alloc &) {
-        cudaStreamSynchronize(st);
         return fail(COLA_ERROR_OUT_OF_MEMORY, "%s: host allocation failed", who);
     }
-    COLA_CUDA(cudaStreamSynchronize(st));
+    COLA_TRY(copy_to_host(jobs, st));
     out = s.release();
     return COLA_SUCCESS;
 }

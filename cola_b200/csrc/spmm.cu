@@ -606,8 +606,11 @@ cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *o
             COLA_TRY(nnz_split(ph.r_colIdx.data(), (int64_t)ph.r_colIdx.size(), ph.r_colPtr.data(),
                                (int64_t)ph.r_rowIdx.size(), sp[(size_t)p].r_col, sp[(size_t)p].r_ptr));
         } else {
-            sp[(size_t)p].r_col = ph.r_colIdx;
-            sp[(size_t)p].r_ptr = ph.r_colIdx.empty() ? std::vector<int32_t>() : ph.r_colPtr;
+            sp[(size_t)p].r_col.assign(ph.r_colIdx.begin(), ph.r_colIdx.end());
+            if (ph.r_colIdx.empty())
+                sp[(size_t)p].r_ptr.clear();
+            else
+                sp[(size_t)p].r_ptr.assign(ph.r_colPtr.begin(), ph.r_colPtr.end());
         }
     }
     // stage tables (pipelined schedule only): work-group column lists are the
