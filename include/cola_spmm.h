@@ -334,7 +334,8 @@ typedef struct cola_spmm_opts {
     int32_t schedule;           /* enum cola_schedule */
     int32_t gather_batch_rows;  /* staging batch (rows) for BUFFER/PIPELINE; 0 = 4096 */
     int32_t unroll;             /* ROWS: row loads in flight per lane group (2, 4, 6 or 8; 0 = 4) */
-    int32_t min_blocks;         /* ROWS: resident blocks per SM the kernel is compiled for (3, 5, 6; 0 = 4) */
+    int32_t min_blocks;         /* ROWS: resident blocks per SM the kernel is compiled for (3, 4, 5, 6;
+                                   0 = 3 for FP32 X, 4 for BF16 X) */
     int32_t reserved[3];
 } cola_spmm_opts;
 
