@@ -603,6 +603,7 @@ def run_batched(args):
             "config": {"workload": BATCHED_DESC, "graphs": len(graphs), "nodes": nodes, "nnz": nnz,
                        "batched_graphs": int(info.batched_graphs), "alg_bytes_per_step": B,
                        "autotuned": {"unroll": int(info.unroll), "grid_pct": int(info.grid_pct),
+                                     "blocks_per_sm": int(info.blocks_per_sm),
                                      "best_ms": tuned_ms},
                        "parallelism": "replicas x{}".format(world),
                        "l2": "inputs larger than L2; no flush", "prep_seconds": round(t_prep, 1)},

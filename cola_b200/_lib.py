@@ -71,7 +71,8 @@ class SpmmOpts(ctypes.Structure):
 
 class BatchInfo(ctypes.Structure):
     _fields_ = [("ngraphs", I32), ("batched_graphs", I32), ("work_items", I64), ("hub_items", I64),
-                ("nnz", I64), ("device_bytes", I64), ("unroll", I32), ("grid_pct", I32), ("last_launches", I64)]
+                ("nnz", I64), ("device_bytes", I64), ("unroll", I32), ("grid_pct", I32), ("blocks_per_sm", I32),
+                ("last_launches", I64)]
 
 
 class ServerOpts(ctypes.Structure):
@@ -129,7 +130,7 @@ SIGNATURES = {
     "cola_batch_run": (I32, [P, P, P]),
     "cola_batch_capture": (I32, [P, P, P]),
     "cola_batch_replay": (I32, [P, P]),
-    "cola_batch_set_params": (I32, [P, I32, I32]),
+    "cola_batch_set_params": (I32, [P, I32, I32, I32]),
     "cola_batch_autotune": (I32, [P, I32, P, P]),
     "cola_batch_get_info": (I32, [P, P]),
     "cola_server_create": (I32, [P, P]),

@@ -64,8 +64,8 @@ class Batch:
     def replay(self, stream=None):
         check(lib().cola_batch_replay(self._h, _stream(stream)))
 
-    def set_params(self, unroll=4, grid_pct=100):
-        check(lib().cola_batch_set_params(self._h, int(unroll), int(grid_pct)))
+    def set_params(self, unroll=4, grid_pct=100, blocks_per_sm=4):
+        check(lib().cola_batch_set_params(self._h, int(unroll), int(grid_pct), int(blocks_per_sm)))
 
     def autotune(self, reps=3, stream=None):
         """Time the launch-parameter candidates on the bound operands; keep the fastest."""

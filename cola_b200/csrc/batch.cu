@@ -40,6 +40,7 @@ struct cola_batch {
     // launch parameters (autotuned)
     int32_t unroll = 4;
     int32_t grid_pct = 100;  // persistent grid as a percentage of one full wave
+    int32_t blocks_per_sm = 4;
     // captured CUDA graph
     cudaGraph_t cgraph = nullptr;
     cudaGraphExec_t cexec = nullptr;
@@ -67,10 +68,10 @@ static void batch_release(cola_batch *b)
     delete b;
 }
 
-template <typename TR, typename TY, int UNROLL>
+template <typename TR, typename TY, int UNROLL, int MINB>
 static cola_status launch_batch_t(const BatchLaunch &L, cudaStream_t st)
 {
-    auto fn = dev::batch_rowblock_kernel<TR, TY, UNROLL>;
+    auto fn = dev::batch_rowblock_kernel<TR, TY, UNROLL, MINB>;
     int64_t gx = grid_for((const void *)fn, L.total_items);
     gx = std::max<int64_t>(1, gx * L.grid_pct / 100);
     t_launches++;
@@ -82,9 +83,9 @@ static cola_status launch_batch_t(const BatchLaunch &L, cudaStream_t st)
 template <typename TR, typename TY>
 static cola_status launch_batch_u(const BatchLaunch &L, cudaStream_t st)
 {
-    if (L.unroll == 2)
-        return launch_batch_t<TR, TY, 2>(L, st);
-    return launch_batch_t<TR, TY, 4>(L, st);
+    if (L.blocks_per_sm == 3)
+        return L.unroll == 2 ? launch_batch_t<TR, TY, 2, 3>(L, st) : launch_batch_t<TR, TY, 4, 3>(L, st);
+    return L.unroll == 2 ? launch_batch_t<TR, TY, 2, 4>(L, st) : launch_batch_t<TR, TY, 4, 4>(L, st);
 }
 
 cola_status launch_batch(const BatchLaunch &L, cudaStream_t st)
@@ -158,6 +159,7 @@ static cola_status batch_run(cola_batch *b, const cola_spmm_opts *opts, cudaStre
     L.ydt = b->ydt;
     L.unroll = b->unroll;
     L.grid_pct = b->grid_pct;
+    L.blocks_per_sm = b->blocks_per_sm;
     L.accumulate = accumulate;
     COLA_TRY(launch_batch(L, st));
     for (const cola_batch::Solo &s : b->solo) {
@@ -323,16 +325,20 @@ cola_status cola_batch_get_info(const cola_batch *b, cola_batch_info *o)
     o->device_bytes += (int64_t)b->d_desc_bytes;
     o->unroll = b->unroll;
     o->grid_pct = b->grid_pct;
+    o->blocks_per_sm = b->blocks_per_sm;
     o->last_launches = b->last_launches;
     return COLA_SUCCESS;
 }
 
-cola_status cola_batch_set_params(cola_batch *b, int32_t unroll, int32_t grid_pct)
+cola_status cola_batch_set_params(cola_batch *b, int32_t unroll, int32_t grid_pct, int32_t blocks_per_sm)
 {
-    COLA_REQUIRE(b && (unroll == 2 || unroll == 4) && grid_pct >= 10 && grid_pct <= 100,
-                 COLA_ERROR_INVALID_ARGUMENT, "cola_batch_set_params: unroll 2 or 4, grid_pct 10..100");
+    COLA_REQUIRE(b && (unroll == 2 || unroll == 4) && grid_pct >= 10 && grid_pct <= 100 &&
+                     (blocks_per_sm == 3 || blocks_per_sm == 4),
+                 COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_batch_set_params: unroll 2 or 4, grid_pct 10..100, blocks_per_sm 3 or 4");
     b->unroll = unroll;
     b->grid_pct = grid_pct;
+    b->blocks_per_sm = blocks_per_sm;
     return COLA_SUCCESS;
 }
 
@@ -346,13 +352,16 @@ cola_status cola_batch_autotune(cola_batch *b, int32_t reps, cola_stream_t strea
     COLA_CUDA(cudaEventCreate(&e1));
     const int32_t unrolls[] = {2, 4};
     const int32_t grids[] = {50, 75, 100};
+    const int32_t occ[] = {3, 4};
     float best = 1e30f;
-    int32_t bu = b->unroll, bg = b->grid_pct;
+    int32_t bu = b->unroll, bg = b->grid_pct, bo = b->blocks_per_sm;
     cola_status s = COLA_SUCCESS;
+    for (int32_t ob : occ)
     for (int32_t u : unrolls)
         for (int32_t gp : grids) {
             b->unroll = u;
             b->grid_pct = gp;
+            b->blocks_per_sm = ob;
             if ((s = batch_run(b, nullptr, st)) != COLA_SUCCESS)  // warm-up
                 goto done;
             cudaEventRecord(e0, st);
@@ -371,11 +380,13 @@ cola_status cola_batch_autotune(cola_batch *b, int32_t reps, cola_stream_t strea
                 best = ms;
                 bu = u;
                 bg = gp;
+                bo = ob;
             }
         }
 done:
     b->unroll = bu;
     b->grid_pct = bg;
+    b->blocks_per_sm = bo;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (s == COLA_SUCCESS && best_ms)

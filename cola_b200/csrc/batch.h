@@ -13,6 +13,7 @@ struct BatchLaunch {
     int64_t total_items, total_hub;
     cola_dtype xdt, ydt;
     int unroll, grid_pct, accumulate;
+    int blocks_per_sm;  // resident blocks per SM the streaming kernel is compiled for: 3 or 4
 };
 
 cola_status launch_batch(const BatchLaunch &L, cudaStream_t st);

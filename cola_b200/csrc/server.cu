@@ -144,6 +144,7 @@ static cola_status launch_group(cola_server *S, Group *G)
     L.ydt = r0->ydt;
     L.unroll = 4;
     L.grid_pct = 100;
+    L.blocks_per_sm = 4;
     L.accumulate = 0;
     COLA_TRY(launch_batch(L, st));
     COLA_CUDA(cudaEventRecord(sl.ev[2], st));

@@ -36,8 +36,8 @@ inline int batch_lane_width(int K, int E)
     return lg;
 }
 
-template <typename TR, typename TY, int UNROLL>
-__global__ void __launch_bounds__(kThreads, 4) batch_rowblock_kernel(const BatchGraph *__restrict__ gs, int ng,
+template <typename TR, typename TY, int UNROLL, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) batch_rowblock_kernel(const BatchGraph *__restrict__ gs, int ng,
                                                                      int64_t total, int accumulate)
 {
     using T = typename ElemOf<TR>::T;

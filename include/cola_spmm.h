@@ -380,18 +380,19 @@ cola_status cola_batch_capture(cola_batch *b, const cola_spmm_opts *opts, cola_s
 cola_status cola_batch_replay(cola_batch *b, cola_stream_t stream);
 
 /* Launch parameters of the batched kernel: loads in flight per lane group (2
- * or 4) and the persistent grid as a percentage of one full wave. */
-cola_status cola_batch_set_params(cola_batch *b, int32_t unroll, int32_t grid_pct);
+ * or 4), the persistent grid as a percentage of one full wave and the resident
+ * blocks per SM it is compiled for (3 or 4). */
+cola_status cola_batch_set_params(cola_batch *b, int32_t unroll, int32_t grid_pct, int32_t blocks_per_sm);
 
 /* The project's autotuner for the batched launch: times every candidate
- * (unroll x grid size) on the bound operands with CUDA events, `reps` runs
+ * (blocks per SM x unroll x grid size) on the bound operands with CUDA events, `reps` runs
  * each, and keeps the fastest (synchronises `stream`). */
 cola_status cola_batch_autotune(cola_batch *b, int32_t reps, cola_stream_t stream, float *best_ms);
 
 typedef struct cola_batch_info {
     int32_t ngraphs, batched_graphs;
     int64_t work_items, hub_items, nnz, device_bytes;
-    int32_t unroll, grid_pct;
+    int32_t unroll, grid_pct, blocks_per_sm;
     int64_t last_launches;
 } cola_batch_info;
 cola_status cola_batch_get_info(const cola_batch *b, cola_batch_info *out);

@@ -75,6 +75,31 @@ def test_batch_capture_replay_and_autotune(graphs):
             assert rel(Y.cpu().numpy(), fp64_reference(n, row, col, val, h)) <= TOL_F32
 
 
+def test_batch_launch_params_do_not_change_results(graphs):
+    # every (blocks per SM, unroll, grid) candidate of the autotuner sums each
+    # row in the same order: bit-identical outputs
+    b = Batch([g[4] for g in graphs])
+    Xs = [torch.from_numpy(dense_x(g[0], K, seed=i)).to(DEV) for i, (g, K) in
+          enumerate(zip(graphs, [16, 32, 64, 128, 256, 64, 32, 128, 16, 64, 128, 32]))]
+    Ys = [torch.zeros((X.shape[0], X.shape[1]), device=DEV) for X in Xs]
+    b.bind(Xs, Ys)
+    outs = []
+    for occ in (3, 4):
+        for unroll in (2, 4):
+            for grid in (50, 100):
+                b.set_params(unroll=unroll, grid_pct=grid, blocks_per_sm=occ)
+                b.run()
+                torch.cuda.synchronize()
+                outs.append([y.clone() for y in Ys])
+                assert b.info.blocks_per_sm == occ and b.info.unroll == unroll
+    for o in outs[1:]:
+        assert all(torch.equal(a, c) for a, c in zip(outs[0], o))
+    for (n, row, col, val, _), Y, X in zip(graphs, outs[0], Xs):
+        assert rel(Y.cpu().numpy(), fp64_reference(n, row, col, val, X.cpu().numpy())) <= TOL_F32
+    with pytest.raises(cb.ColaError):
+        b.set_params(unroll=4, grid_pct=100, blocks_per_sm=5)
+
+
 def test_batch_bf16(graphs):
     b = Batch([g[4] for g in graphs[:6]])
     Xs, Ys, refs = [], [], []
