@@ -65,6 +65,24 @@ def alg_bytes(nnz, M, K, s_x, s_y, s_v=4):
     return nnz * (4 + s_v + K * s_x) + (M + 1) * 4 + M * K * s_y
 
 
+def world_reduce(x, dev, op="max"):
+    """x reduced over the ranks of the default process group (max or sum);
+    x itself when there is one rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def world_barrier():
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.barrier()
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -318,15 +336,10 @@ def run_ours(args, w):
         g.spmm(X, Y, schedule=sched, unroll=args.unroll, min_blocks=args.min_blocks, stream=stream)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        world_barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return world_reduce(x, dev, "max")
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -554,6 +567,8 @@ def run_batched(args):
     for _ in range(max(args.warmup, 3)):
         b.replay(stream)
     torch.cuda.synchronize()
+    world_barrier()
+    torch.cuda.synchronize()
     clocks = Clocks(local)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -563,11 +578,7 @@ def run_batched(args):
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = world_reduce(e0.elapsed_time(e1) / args.steps, dev, "max")
     # e2e: per graph pinned X -> device, the captured launch, Y -> pinned host
     e2e_ms = None
     if not args.no_e2e:
@@ -687,6 +698,7 @@ def run_serving(args):
         submit(*draw()).wait()
     for r in [submit(*draw()) for _ in range(args.serve_burst)]:
         r.wait()
+    world_barrier()
     burst = [draw() for _ in range(args.serve_burst)]
     tb = time.perf_counter()
     reqs = [submit(*d) for d in burst]
@@ -717,11 +729,7 @@ def run_serving(args):
     st = srv.stats()
     B = sum(req_bytes(*d) for d in plan)
     h2d = sum(gn[g] * K * (4 if dt == torch.float32 else 2) for g, K, dt in plan) / nreq
-    value = B / wall / 1e9
-    if world > 1:
-        t = torch.tensor([value], dtype=torch.float64, device=dev)
-        dist.all_reduce(t)
-        value = float(t.item())
+    value = world_reduce(B / wall / 1e9, dev, "sum")
     peak, peak_kind = measured_peak()
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": nreq,
             "warmup": max(args.warmup, 3), "ms_per_step": wall * 1e3 / nreq, "higher_is_better": True,
@@ -826,8 +834,7 @@ def run_prep(args):
     for _ in range(max(args.warmup, 3)):
         build(rd, cd, vd).close()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    world_barrier()
     clocks = Clocks(local)
     clocks.start()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -836,12 +843,8 @@ def run_prep(args):
         build(rd, cd, vd).close()
     ev[1].record(stream)
     torch.cuda.synchronize()
-    ms = ev[0].elapsed_time(ev[1]) / args.steps
     clk = clocks.stop()
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = world_reduce(ev[0].elapsed_time(ev[1]) / args.steps, dev, "max")
     # end to end: pinned host COO -> device, build, partitions in host memory
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2e_steps = max(1, min(args.steps, 5))
