@@ -70,6 +70,9 @@ struct cola_graph {
     int64_t last_launches = 0;       // kernels launched by the last cola_spmm call
     GatherSeg *d_bufsegs = nullptr;  // BUFFER schedule gather segments
     std::vector<GatherSeg> h_bufsegs;
+    // the split local CSR / remote CSC blocks (FUSED, BUFFER, PIPELINE, zip
+    // views); false for a graph built on the device, which has the row view only
+    bool has_split = true;
     // row-major view (ROWS schedule): merged local + transposed remote entries
     bool has_rows = false;
     const int64_t *rv_ptr = nullptr;  // N+1

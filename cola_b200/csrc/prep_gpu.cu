@@ -386,6 +386,151 @@ __global__ void relabel_kernel(const int32_t *row, const int32_t *col, int64_t n
 }
 
 // ---------------------------------------------------------------------------
+// row view of a graph built on the device: the global CSR (row, col) order of
+// the unique entries, hub segments and row-block tasks, the same arrays the
+// host upload derives from the partitions (spmm.cu graph_upload)
+// ---------------------------------------------------------------------------
+
+__global__ void make_row_keys_kernel(const int32_t *row, const int32_t *col, int64_t n, int cb, uint64_t *key,
+                                     uint32_t *idx)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        key[i] = (uint64_t)(uint32_t)row[i] << cb | (uint32_t)col[i];
+        idx[i] = (uint32_t)i;
+    }
+}
+
+// rv_ptr[r] = first unique entry of row >= r (r = 0..N); rv_col = the columns
+__global__ void row_ptr_kernel(const uint64_t *ukey, int64_t U, int cb, int64_t N, int64_t *rv_ptr)
+{
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= N; r += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t kb = (uint64_t)r << cb;
+        int64_t lo = 0, hi = U;
+        while (lo < hi) {
+            const int64_t m = (lo + hi) >> 1;
+            if (ukey[m] < kb)
+                lo = m + 1;
+            else
+                hi = m;
+        }
+        rv_ptr[r] = lo;
+    }
+}
+
+__global__ void row_cols_kernel(const uint64_t *ukey, int64_t U, uint64_t cmask, int32_t *rv_col)
+{
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < U; u += (int64_t)gridDim.x * blockDim.x)
+        rv_col[u] = (int32_t)(ukey[u] & cmask);
+}
+
+// 1 per hub row (more than thr entries)
+struct HubF {
+    const int64_t *ptr;
+    int64_t thr;
+    __device__ uint32_t operator()(int64_t r) const { return ptr[r + 1] - ptr[r] > thr; }
+};
+// segments of row r: ceil(len / seg) for a hub row, else 0
+struct SegCountF {
+    const int64_t *ptr;
+    int64_t thr, seg;
+    __device__ uint32_t operator()(int64_t r) const
+    {
+        const int64_t len = ptr[r + 1] - ptr[r];
+        return len > thr ? (uint32_t)((len + seg - 1) / seg) : 0u;
+    }
+};
+// 1 where a run of non-hub rows starts
+struct RunStartF {
+    const int64_t *ptr;
+    int64_t thr;
+    __device__ uint32_t operator()(int64_t r) const
+    {
+        const bool hub = ptr[r + 1] - ptr[r] > thr;
+        return !hub && (r == 0 || ptr[r] - ptr[r - 1] > thr);
+    }
+};
+
+__global__ void hub_segments_kernel(const int64_t *ptr, int64_t N, int64_t thr, int64_t seg, const uint32_t *hubpos,
+                                    const uint32_t *segoff, int64_t nhub, int64_t nseg, int32_t *hub_row,
+                                    int64_t *hub_seg, int32_t *seg_row, int64_t *seg_beg)
+{
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = ptr[r], e = ptr[r + 1];
+        if (e - b <= thr)
+            continue;
+        const int64_t h = hubpos[r], s0 = segoff[r];
+        hub_row[h] = (int32_t)r;
+        hub_seg[h] = s0;
+        int64_t s = s0;
+        for (int64_t q = b; q < e; q += seg, s++) {
+            seg_row[s] = (int32_t)r;
+            seg_beg[s] = q;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        hub_seg[nhub] = nseg;
+}
+
+// The host's greedy packing of rows into tasks (a row costs its entries plus
+// 2; a task closes once its cost reaches te; hub rows close a task and belong
+// to none), run independently on every run of non-hub rows, which is exactly
+// where the greedy state is reset.  Pass 1 (rb == nullptr) counts each run's
+// tasks into cnt; pass 2 writes them from off[run] on.
+__global__ void run_tasks_kernel(const int64_t *ptr, int64_t N, int64_t thr, int64_t te, const uint32_t *runpos,
+                                 uint32_t *cnt, const uint32_t *off, int32_t *rb, int32_t *re)
+{
+    for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < N; a += (int64_t)gridDim.x * blockDim.x) {
+        const bool hub_a = ptr[a + 1] - ptr[a] > thr;
+        if (hub_a || (a > 0 && !(ptr[a] - ptr[a - 1] > thr)))
+            continue;  // not the first row of a run
+        const uint32_t run = runpos[a];
+        uint32_t t = rb ? off[run] : 0u, k = 0;
+        int64_t start = -1, cost = 0, r = a;
+        for (; r < N; r++) {
+            const int64_t len = ptr[r + 1] - ptr[r];
+            if (len > thr)
+                break;
+            if (start < 0)
+                start = r;
+            cost += len + 2;
+            if (cost >= te) {
+                if (rb) {
+                    rb[t + k] = (int32_t)start;
+                    re[t + k] = (int32_t)(r + 1);
+                }
+                k++;
+                start = -1;
+                cost = 0;
+            }
+        }
+        if (start >= 0) {
+            if (rb) {
+                rb[t + k] = (int32_t)start;
+                re[t + k] = (int32_t)r;
+            }
+            k++;
+        }
+        if (!rb)
+            cnt[run] = k;
+    }
+}
+
+// entries whose column lies in the row's own partition (the local block)
+__global__ void count_local_kernel(const uint64_t *ukey, int64_t U, int cb, uint32_t npp,
+                                   unsigned long long *local)
+{
+    unsigned long long c = 0;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < U; u += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = (uint32_t)(ukey[u] >> cb), k = (uint32_t)(ukey[u] & ((1ull << cb) - 1));
+        c += r / npp == k / npp;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c)
+        atomicAdd(local, c);
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 
@@ -575,6 +720,26 @@ static cola_status check_range(const int32_t *row, const int32_t *col, int64_t n
     return COLA_SUCCESS;
 }
 
+// Stable LSD radix sort of (key, id) pairs by the low key_bits bits of the
+// keys: on return k0/v0 point at the sorted pairs, k1/v1 at the other buffers.
+static cola_status radix_sort_pairs(uint64_t *&k0, uint32_t *&v0, uint64_t *&k1, uint32_t *&v1, int64_t n,
+                                    int key_bits, uint32_t *hist, uint32_t *d_total, Scratch &sc)
+{
+    const int64_t ntiles = (n + kTile - 1) / kTile;
+    for (int shift = 0; shift < key_bits; shift += kDigitBits) {
+        radix_hist_kernel<<<(unsigned)ntiles, kThreads, 0, sc.st>>>(k0, n, shift, ntiles, hist);
+        t_launches++;
+        COLA_CUDA(cudaGetLastError());
+        COLA_TRY(exclusive_scan(ArrayF{hist}, ntiles * kBins, hist, d_total, nullptr, sc));
+        radix_scatter_kernel<<<(unsigned)ntiles, kThreads, 0, sc.st>>>(k0, v0, k1, v1, n, shift, ntiles, hist);
+        t_launches++;
+        COLA_CUDA(cudaGetLastError());
+        std::swap(k0, k1);
+        std::swap(v0, v1);
+    }
+    return COLA_SUCCESS;
+}
+
 static cola_status partition_build_device(int32_t N, int64_t nnz, const int32_t *row, const int32_t *col,
                                           const float *val, int32_t nparts, cudaStream_t st, cola_partition_set *&out)
 {
@@ -636,17 +801,7 @@ static cola_status partition_build_device(int32_t N, int64_t nnz, const int32_t 
                                                               gshift, k0, v0);
     t_launches++;
     COLA_CUDA(cudaGetLastError());
-    for (int shift = 0; shift < key_bits; shift += kDigitBits) {
-        radix_hist_kernel<<<(unsigned)ntiles, kThreads, 0, st>>>(k0, nnz, shift, ntiles, hist);
-        t_launches++;
-        COLA_CUDA(cudaGetLastError());
-        COLA_TRY(exclusive_scan(ArrayF{hist}, ntiles * kBins, hist, d_total, nullptr, sc));
-        radix_scatter_kernel<<<(unsigned)ntiles, kThreads, 0, st>>>(k0, v0, k1, v1, nnz, shift, ntiles, hist);
-        t_launches++;
-        COLA_CUDA(cudaGetLastError());
-        std::swap(k0, k1);
-        std::swap(v0, v1);
-    }
+    COLA_TRY(radix_sort_pairs(k0, v0, k1, v1, nnz, key_bits, hist, d_total, sc));
     // merge duplicates: unique keys into k1, summed values
     uint32_t *upos = nullptr;
     float *uval = nullptr;
@@ -718,6 +873,184 @@ static cola_status partition_build_device(int32_t N, int64_t nnz, const int32_t 
     return COLA_SUCCESS;
 }
 
+// The row view of cola_graph_upload, built from a device COO without the
+// host: entries sorted by (row, col) with duplicates merged (values summed in
+// input order), row pointers, hub segments and row-block tasks.  The result is
+// identical to the upload of the same COO's partitions, array for array.
+static cola_status graph_build_device(int32_t N, int64_t nnz, const int32_t *row, const int32_t *col,
+                                      const float *val, int32_t nparts, const cola_upload_opts *opts, cudaStream_t st,
+                                      cola_graph *&out)
+{
+    const char *who = "cola_graph_build_device";
+    COLA_REQUIRE(N >= 0 && nnz >= 0 && nparts >= 1, COLA_ERROR_INVALID_ARGUMENT, "%s: N=%d nnz=%lld nparts=%d", who,
+                 N, (long long)nnz, nparts);
+    COLA_REQUIRE(nnz == 0 || (row && col), COLA_ERROR_INVALID_ARGUMENT, "%s: null COO arrays", who);
+    COLA_REQUIRE(nnz < (int64_t)UINT32_MAX, COLA_ERROR_UNSUPPORTED, "%s: nnz >= 2^32", who);
+    COLA_REQUIRE(!(opts && opts->no_row_view), COLA_ERROR_INVALID_ARGUMENT,
+                 "%s: a graph built on the device is its row view", who);
+    COLA_REQUIRE(!(opts && opts->group_size > 0 && opts->group_size != nparts), COLA_ERROR_UNSUPPORTED,
+                 "%s: the pipelined schedule needs the split blocks (cola_graph_upload)", who);
+    const int64_t thr = opts && opts->hub_threshold > 0 ? opts->hub_threshold : 256;
+    const int64_t seg = opts && opts->hub_segment > 0 ? opts->hub_segment : 256;
+    const int64_t te = opts && opts->task_entries > 0 ? opts->task_entries : 128;
+    const int64_t npp = ((int64_t)N + nparts - 1) / nparts;
+    const int cb = bits_for(N > 0 ? (uint64_t)N - 1 : 0);
+
+    std::unique_ptr<cola_graph, void (*)(cola_graph *)> g(new (std::nothrow) cola_graph(), graph_release);
+    COLA_REQUIRE(g, COLA_ERROR_OUT_OF_MEMORY, "%s: host allocation failed", who);
+    COLA_CUDA(cudaGetDevice(&g->device));
+    g->N = N;
+    g->P = nparts;
+    g->npp = (int32_t)npp;
+    g->gs = nparts;
+    g->nstages = 1;
+    g->has_split = false;
+    g->hub_threshold = (int32_t)thr;
+    g->hub_segment = (int32_t)seg;
+    g->task_entries = (int32_t)te;
+
+    Scratch sc(st);
+    {
+        const size_t n = (size_t)nnz, a = 256;
+        const int64_t ntiles = (nnz + kTile - 1) / kTile;
+        const size_t rows = (size_t)N + 1;
+        const size_t scan_blocks = (size_t)((std::max<int64_t>(std::max<int64_t>(ntiles * kBins, nnz), N + 1) +
+                                             kScanTile - 1) / kScanTile) + 1;
+        // sort keys and ids (x2), digit counts, unique positions, values and
+        // columns, row pointers, hub / segment / run positions, run task
+        // counts and offsets, small values, the scans' block sums
+        const size_t bytes = 2 * (8 * n + a) + 2 * (4 * n + a) + (4 * (size_t)ntiles * kBins + a) + 3 * (4 * n + a) +
+                             (8 * rows + a) + 5 * (4 * rows + a) + 4 * a + 24 * (4 * scan_blocks + a);
+        COLA_TRY(sc.reserve(bytes));
+    }
+    if (nnz > 0)
+        COLA_TRY(check_range(row, col, nnz, N, sc, who));
+    uint32_t *d_total = nullptr;
+    COLA_TRY(sc.get(d_total, 1));
+    uint64_t *ukey = nullptr;
+    float *uval = nullptr;
+    uint32_t U = 0;
+    if (nnz > 0) {
+        uint64_t *k0 = nullptr, *k1 = nullptr;
+        uint32_t *v0 = nullptr, *v1 = nullptr, *hist = nullptr, *upos = nullptr;
+        const int64_t ntiles = (nnz + kTile - 1) / kTile;
+        COLA_TRY(sc.get(k0, nnz));
+        COLA_TRY(sc.get(k1, nnz));
+        COLA_TRY(sc.get(v0, nnz));
+        COLA_TRY(sc.get(v1, nnz));
+        COLA_TRY(sc.get(hist, ntiles * kBins));
+        make_row_keys_kernel<<<grid_stride_blocks(nnz), 256, 0, st>>>(row, col, nnz, cb, k0, v0);
+        t_launches++;
+        COLA_CUDA(cudaGetLastError());
+        COLA_TRY(radix_sort_pairs(k0, v0, k1, v1, nnz, 2 * cb, hist, d_total, sc));
+        COLA_TRY(sc.get(upos, nnz));
+        COLA_TRY(exclusive_scan(KeyStartF{k0, 0}, nnz, upos, d_total, &U, sc));
+        COLA_TRY(sc.get(uval, U));
+        ukey = k1;
+        dedupe_kernel<<<grid_stride_blocks(nnz), 256, 0, st>>>(k0, v0, val, nnz, upos, ukey, uval);
+        t_launches++;
+        COLA_CUDA(cudaGetLastError());
+    }
+    // row pointers and columns
+    int64_t *rv_ptr = nullptr;
+    int32_t *rv_col = nullptr;
+    COLA_TRY(sc.get(rv_ptr, (int64_t)N + 1));
+    COLA_TRY(sc.get(rv_col, U));
+    if (U > 0) {
+        row_ptr_kernel<<<grid_stride_blocks((int64_t)N + 1), 256, 0, st>>>(ukey, U, cb, N, rv_ptr);
+        row_cols_kernel<<<grid_stride_blocks(U), 256, 0, st>>>(ukey, U, cb >= 64 ? ~0ull : (1ull << cb) - 1, rv_col);
+        t_launches += 2;
+    } else {
+        COLA_CUDA(cudaMemsetAsync(rv_ptr, 0, ((size_t)N + 1) * 8, st));
+    }
+    COLA_CUDA(cudaGetLastError());
+    // hub rows and their segments; runs of non-hub rows and their tasks
+    uint32_t nhub = 0, nseg = 0, nrun = 0, ntask = 0;
+    uint32_t *hubpos = nullptr, *segoff = nullptr, *runpos = nullptr, *cnt = nullptr, *toff = nullptr;
+    COLA_TRY(sc.get(hubpos, N));
+    COLA_TRY(sc.get(segoff, N));
+    COLA_TRY(sc.get(runpos, N));
+    COLA_TRY(exclusive_scan(HubF{rv_ptr, thr}, N, hubpos, d_total, &nhub, sc));
+    COLA_TRY(exclusive_scan(SegCountF{rv_ptr, thr, seg}, N, segoff, d_total, &nseg, sc));
+    COLA_TRY(exclusive_scan(RunStartF{rv_ptr, thr}, N, runpos, d_total, &nrun, sc));
+    COLA_TRY(sc.get(cnt, nrun));
+    COLA_TRY(sc.get(toff, nrun));
+    if (nrun > 0) {
+        run_tasks_kernel<<<grid_stride_blocks(N), 256, 0, st>>>(rv_ptr, N, thr, te, runpos, cnt, nullptr, nullptr,
+                                                                nullptr);
+        t_launches++;
+        COLA_CUDA(cudaGetLastError());
+        COLA_TRY(exclusive_scan(ArrayF{cnt}, nrun, toff, d_total, &ntask, sc));
+    }
+    // nnz in the partitions' local blocks
+    unsigned long long *d_local = nullptr, h_local = 0;
+    COLA_TRY(sc.get(d_local, 1));
+    COLA_CUDA(cudaMemsetAsync(d_local, 0, sizeof(*d_local), st));
+    if (U > 0) {
+        count_local_kernel<<<grid_stride_blocks(U), 256, 0, st>>>(ukey, U, cb, (uint32_t)std::max<int64_t>(npp, 1),
+                                                                  d_local);
+        t_launches++;
+    }
+    COLA_CUDA(cudaMemcpyAsync(&h_local, d_local, sizeof(h_local), cudaMemcpyDeviceToHost, st));
+
+    // the graph's own arena, in the order and alignment of the host upload
+    size_t total = 0;
+    auto place = [&](size_t bytes) {
+        const size_t o = total;
+        total += (bytes + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_ptr = place(((size_t)N + 1) * 8), o_col = place((size_t)U * 4), o_val = place((size_t)U * 4);
+    const size_t o_srow = place((size_t)nseg * 4), o_sbeg = place((size_t)nseg * 8);
+    const size_t o_hrow = place((size_t)nhub * 4), o_hseg = place(((size_t)nhub + 1) * 8);
+    const size_t o_trb = place((size_t)ntask * 4), o_tre = place((size_t)ntask * 4);
+    total = std::max<size_t>(total, 256);
+    COLA_CUDA(cudaMalloc(&g->dmem, total));
+    g->dbytes = total;
+    char *base = static_cast<char *>(g->dmem);
+    COLA_CUDA(cudaMemcpyAsync(base + o_ptr, rv_ptr, ((size_t)N + 1) * 8, cudaMemcpyDeviceToDevice, st));
+    if (U > 0) {
+        COLA_CUDA(cudaMemcpyAsync(base + o_col, rv_col, (size_t)U * 4, cudaMemcpyDeviceToDevice, st));
+        COLA_CUDA(cudaMemcpyAsync(base + o_val, uval, (size_t)U * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    const int64_t *ptr_final = reinterpret_cast<const int64_t *>(base + o_ptr);
+    if (N > 0) {
+        hub_segments_kernel<<<grid_stride_blocks(N), 256, 0, st>>>(
+            ptr_final, N, thr, seg, hubpos, segoff, nhub, nseg, reinterpret_cast<int32_t *>(base + o_hrow),
+            reinterpret_cast<int64_t *>(base + o_hseg), reinterpret_cast<int32_t *>(base + o_srow),
+            reinterpret_cast<int64_t *>(base + o_sbeg));
+        t_launches++;
+        if (nrun > 0) {
+            run_tasks_kernel<<<grid_stride_blocks(N), 256, 0, st>>>(ptr_final, N, thr, te, runpos, nullptr, toff,
+                                                                    reinterpret_cast<int32_t *>(base + o_trb),
+                                                                    reinterpret_cast<int32_t *>(base + o_tre));
+            t_launches++;
+        }
+        COLA_CUDA(cudaGetLastError());
+    } else {
+        const int64_t zero = 0;
+        COLA_CUDA(cudaMemcpyAsync(base + o_hseg, &zero, 8, cudaMemcpyHostToDevice, st));
+    }
+    COLA_CUDA(cudaStreamSynchronize(st));
+    g->has_rows = true;
+    g->rv_ptr = ptr_final;
+    g->rv_col = reinterpret_cast<const int32_t *>(base + o_col);
+    g->rv_val = reinterpret_cast<const float *>(base + o_val);
+    g->seg_row = reinterpret_cast<const int32_t *>(base + o_srow);
+    g->seg_beg = reinterpret_cast<const int64_t *>(base + o_sbeg);
+    g->hub_row = reinterpret_cast<const int32_t *>(base + o_hrow);
+    g->hub_seg = reinterpret_cast<const int64_t *>(base + o_hseg);
+    g->task_rb = reinterpret_cast<const int32_t *>(base + o_trb);
+    g->task_re = reinterpret_cast<const int32_t *>(base + o_tre);
+    g->nseg = nseg;
+    g->nhub = nhub;
+    g->ntask = ntask;
+    g->nnz_l = (int64_t)h_local;
+    g->nnz_r = (int64_t)U - (int64_t)h_local;
+    out = g.release();
+    return COLA_SUCCESS;
+}
+
 }  // namespace pg
 }  // namespace cola
 
@@ -735,6 +1068,19 @@ cola_status cola_partition_build_device(int32_t num_nodes, int64_t nnz, const in
     cola_partition_set *s = nullptr;
     COLA_TRY(pg::partition_build_device(num_nodes, nnz, row, col, val, nparts, stream, s));
     *out = s;
+    return COLA_SUCCESS;
+}
+
+cola_status cola_graph_build_device(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
+                                    const float *val, int32_t nparts, const cola_upload_opts *opts,
+                                    cudaStream_t stream, cola_graph **out)
+{
+    COLA_REQUIRE(out, COLA_ERROR_INVALID_ARGUMENT, "cola_graph_build_device: out is NULL");
+    *out = nullptr;
+    clear_error();
+    cola_graph *g = nullptr;
+    COLA_TRY(pg::graph_build_device(num_nodes, nnz, row, col, val, nparts, opts, stream, g));
+    *out = g;
     return COLA_SUCCESS;
 }
 

@@ -987,6 +987,8 @@ cola_status cola_graph_zip_view(const cola_graph *g, int32_t part, cola_zip_view
 {
     COLA_REQUIRE(g && o && part >= 0 && part < g->P, COLA_ERROR_INVALID_ARGUMENT,
                  "cola_graph_zip_view: bad argument (part %d)", part);
+    COLA_REQUIRE(g->has_split, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_graph_zip_view: a graph built on the device has no split blocks");
     *o = g->zips[(size_t)part];
     return COLA_SUCCESS;
 }
@@ -1022,6 +1024,8 @@ static cola_status spmm_impl(cola_graph *g, const void *X, cola_dtype xdt, int64
         schedule = g->has_rows ? COLA_SCHEDULE_ROWS : (g->nstages > 1 ? COLA_SCHEDULE_PIPELINE : COLA_SCHEDULE_FUSED);
     COLA_REQUIRE(schedule != COLA_SCHEDULE_ROWS || g->has_rows, COLA_ERROR_INVALID_ARGUMENT,
                  "cola_spmm: the row-major schedule needs a graph uploaded with its row view");
+    COLA_REQUIRE(schedule == COLA_SCHEDULE_ROWS || g->has_split, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_spmm: a graph built on the device has the row-major schedule only");
     COLA_REQUIRE(schedule >= COLA_SCHEDULE_FUSED && schedule <= COLA_SCHEDULE_ROWS, COLA_ERROR_INVALID_ARGUMENT,
                  "cola_spmm: unknown schedule %d", schedule);
     COLA_REQUIRE(schedule != COLA_SCHEDULE_PIPELINE || g->nstages > 1, COLA_ERROR_INVALID_ARGUMENT,

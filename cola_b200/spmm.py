@@ -60,6 +60,35 @@ class Graph:
         self.nparts = self.info.nparts
         self.nodes_per_part = self.info.nodes_per_part
 
+    @classmethod
+    def from_coo_device(cls, num_nodes, row, col, val=None, nparts=1, hub_threshold=0, hub_segment=0,
+                        task_entries=0, stream=None):
+        """The graph built on the GPU straight from a COO in CUDA tensors
+        (int32 row/col, optional float32 val): the row view only (the
+        row-major schedule), identical to Graph(PartitionSet.from_coo(...))'s."""
+        for t, name in ((row, "row"), (col, "col")):
+            if not t.is_cuda or t.dtype != torch.int32 or not t.is_contiguous():
+                raise ValueError("{} must be a contiguous int32 CUDA tensor".format(name))
+        if row.numel() != col.numel() or (val is not None and val.numel() != row.numel()):
+            raise ValueError("row, col and val differ in length")
+        if val is not None and (not val.is_cuda or val.dtype != torch.float32 or not val.is_contiguous()):
+            raise ValueError("val must be a contiguous float32 CUDA tensor")
+        o = UploadOpts()
+        o.if_split = 1
+        o.hub_threshold = int(hub_threshold)
+        o.hub_segment = int(hub_segment)
+        o.task_entries = int(task_entries)
+        h = ctypes.c_void_p()
+        check(lib().cola_graph_build_device(int(num_nodes), row.numel(), _ptr(row), _ptr(col), _ptr(val),
+                                            int(nparts), ctypes.byref(o), _stream(stream), ctypes.byref(h)))
+        g = cls.__new__(cls)
+        g._h = h
+        g.info = g.get_info()
+        g.num_nodes = g.info.num_nodes
+        g.nparts = g.info.nparts
+        g.nodes_per_part = g.info.nodes_per_part
+        return g
+
     def get_info(self):
         i = GraphInfo()
         check(lib().cola_graph_get_info(self._h, ctypes.byref(i)))

@@ -296,6 +296,20 @@ cola_status cola_graph_upload(const cola_partition_set *parts, const cola_upload
                               cola_stream_t stream);
 cola_status cola_graph_free(cola_graph *g);
 
+/* A graph for the row-major schedule (COLA_SCHEDULE_ROWS, what AUTO picks)
+ * built straight from the COO in device memory: entries sorted by (row, col)
+ * with duplicates merged, row pointers, hub segments and row-block tasks, all
+ * on the device, identical to what cola_graph_upload derives from the
+ * partitions of the same COO (so every SpMM gives the same bits).  It has no
+ * split blocks: the FUSED, BUFFER and PIPELINE schedules and
+ * cola_graph_zip_view refuse it.  opts: hub_threshold, hub_segment and
+ * task_entries as for cola_graph_upload (may be NULL).  Free with
+ * cola_graph_free. */
+cola_status cola_graph_build_device(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
+                                    const float *val, int32_t nparts, const cola_upload_opts *opts,
+                                    cola_stream_t stream, cola_graph **out);
+
+
 typedef struct cola_graph_info {
     int32_t num_nodes, nparts, nodes_per_part, group_size;
     int64_t nnz, nnz_local, nnz_remote;

@@ -161,3 +161,63 @@ def test_relabelled_graph_spmm_is_the_permuted_product():
     Yp = S.Graph(ps).spmm(torch.from_numpy(Xp).to(DEV)).cpu().numpy()
     ref = fp64_reference(n, row, col, val, X)
     assert rel(Yp[mapping], ref) <= TOL_F32
+
+
+# ---------------------------------------------------------------------------
+# the whole graph built on the device (row view, hub segments, tasks)
+# ---------------------------------------------------------------------------
+def device_graph(n, row, col, val, P, **kw):
+    return S.Graph.from_coo_device(n, dev(row), dev(col), None if val is None else dev(val, torch.float32), P, **kw)
+
+
+@pytest.mark.parametrize("scale,deg,P,thr,seg,te", [(12, 16, 4, 0, 0, 0), (11, 8, 3, 8, 4, 64), (13, 24, 8, 32, 16, 300),
+                                                    (10, 4, 1, 10 ** 6, 256, 1), (12, 16, 16, 1, 1, 0)])
+def test_device_graph_equals_uploaded_graph(scale, deg, P, thr, seg, te):
+    """Same statistics as the host upload of the same COO's partitions, and
+    bit-identical SpMM results for every width (narrow widths interleave
+    entries over lane groups relative to each task's start, so equal bits
+    mean equal tasks and hub segments too)."""
+    n, row, col, val = cb.rmat(scale, deg, seed=scale + P)
+    keep = n - 5
+    m = (row < keep) & (col < keep)
+    row, col, val = with_duplicates(keep, row[m], col[m], val[m], seed=P)
+    kw = dict(hub_threshold=thr, hub_segment=seg, task_entries=te)
+    gd = device_graph(keep, row, col, val, P, **kw)
+    gh = S.Graph(cb.PartitionSet.from_coo(keep, row, col, val, P), **kw)
+    di, hi = gd.info, gh.info
+    for k in ("num_nodes", "nparts", "nodes_per_part", "nnz", "nnz_local", "nnz_remote", "hub_rows", "hub_segments",
+              "row_tasks"):
+        assert getattr(di, k) == getattr(hi, k), k
+    for K, xdt, ydt in [(8, torch.float32, torch.float32), (16, torch.float32, torch.float32),
+                        (64, torch.float32, torch.float32), (128, torch.float32, torch.float32),
+                        (256, torch.bfloat16, torch.bfloat16), (32, torch.bfloat16, torch.float32)]:
+        X = torch.from_numpy(dense_x(keep, K, seed=K)).to(DEV).to(xdt)
+        yd = gd.spmm(X, out_dtype=ydt)
+        yh = gh.spmm(X, out_dtype=ydt, schedule=S.SCHEDULE_ROWS)
+        torch.cuda.synchronize()
+        assert torch.equal(yd, yh), (K, xdt, ydt)
+    ref = fp64_reference(keep, row, col, val, dense_x(keep, 64, seed=64))
+    y = gd.spmm(torch.from_numpy(dense_x(keep, 64, seed=64)).to(DEV))
+    assert rel(y.cpu().numpy(), ref) <= TOL_F32
+
+
+def test_device_graph_is_rows_only_and_edge_cases():
+    n, row, col, val = cb.rmat(10, 8, seed=1)
+    g = device_graph(n, row, col, val, 4)
+    X = torch.ones((n, 16), device=DEV)
+    for sched in (S.SCHEDULE_FUSED, S.SCHEDULE_BUFFER):
+        with pytest.raises(cb.ColaError, match="row-major"):
+            g.spmm(X, schedule=sched)
+    with pytest.raises(cb.ColaError):
+        g.zip_view(0)
+    # no entries: Y is all zeros; rows of a one-node graph
+    e = torch.zeros(0, dtype=torch.int32, device=DEV)
+    g0 = S.Graph.from_coo_device(50, e, e, None, 3)
+    assert g0.info.nnz == 0 and g0.info.row_tasks > 0
+    y0 = g0.spmm(torch.ones((50, 32), device=DEV))
+    g1 = device_graph(1, np.array([0, 0], np.int32), np.array([0, 0], np.int32), np.array([0.5, 2.0], np.float32), 2)
+    y1 = g1.spmm(torch.full((1, 8), 3.0, device=DEV))
+    torch.cuda.synchronize()
+    assert torch.all(y0 == 0) and torch.all(y1 == 7.5)
+    with pytest.raises(cb.ColaError, match="entry 1"):
+        device_graph(4, np.array([0, 4], np.int32), np.array([1, 1], np.int32), None, 2)
