@@ -126,6 +126,7 @@ SIGNATURES = {
     "cola_graph_zip_view": (I32, [P, I32, P]),
     "cola_spmm": (I32, [P, P, I32, I64, P, I32, I64, I32, P, P]),
     "cola_batch_create": (I32, [P, I32, P, P, P]),
+    "cola_batch_create_from_graphs": (I32, [P, I32, P]),
     "cola_batch_free": (I32, [P]),
     "cola_batch_bind": (I32, [P, P, P, P, P, P, I32, I32, P]),
     "cola_batch_run": (I32, [P, P, P]),
@@ -137,6 +138,7 @@ SIGNATURES = {
     "cola_server_create": (I32, [P, P]),
     "cola_server_destroy": (I32, [P]),
     "cola_server_register": (I32, [P, P, P, P]),
+    "cola_server_register_graph": (I32, [P, P, P]),
     "cola_server_submit": (I32, [P, I32, P, I32, I32, P, I32, P]),
     "cola_server_wait": (I32, [P, ctypes.c_uint64, I32]),
     "cola_server_cancel": (I32, [P, ctypes.c_uint64]),

@@ -26,6 +26,21 @@ class Batch:
         self.num_nodes = [p.num_nodes for p in psets]
         self._bound = None
 
+    @classmethod
+    def from_graphs(cls, graphs):
+        """A batch over existing Graph objects (uploaded with their row view, or
+        built on the device); the batch keeps them alive and borrows them."""
+        arr = (ctypes.c_void_p * max(len(graphs), 1))(*[g._h.value for g in graphs])
+        h = ctypes.c_void_p()
+        check(lib().cola_batch_create_from_graphs(arr, len(graphs), ctypes.byref(h)))
+        b = cls.__new__(cls)
+        b._h = h
+        b.ngraphs = len(graphs)
+        b.num_nodes = [g.num_nodes for g in graphs]
+        b._bound = None
+        b._graphs = list(graphs)
+        return b
+
     def bind(self, Xs, Ys, stream=None):
         """Bind per-graph dense operands (CUDA tensors; all X one dtype, all Y one dtype)."""
         if len(Xs) != self.ngraphs or len(Ys) != self.ngraphs:

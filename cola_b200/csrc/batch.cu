@@ -204,6 +204,31 @@ cola_status cola_batch_create(const cola_partition_set *const *parts, int32_t ng
     return COLA_SUCCESS;
 }
 
+cola_status cola_batch_create_from_graphs(cola_graph *const *graphs, int32_t ngraphs, cola_batch **out)
+{
+    COLA_REQUIRE(out && (ngraphs == 0 || graphs) && ngraphs >= 0, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_batch_create_from_graphs: bad argument");
+    *out = nullptr;
+    std::unique_ptr<cola_batch, void (*)(cola_batch *)> b(new (std::nothrow) cola_batch(), batch_release);
+    COLA_REQUIRE(b, COLA_ERROR_OUT_OF_MEMORY, "cola_batch_create_from_graphs: host allocation failed");
+    b->own_graphs = false;
+    COLA_CUDA(cudaGetDevice(&b->device));
+    for (int32_t i = 0; i < ngraphs; i++) {
+        COLA_REQUIRE(graphs[i] && graphs[i]->has_rows, COLA_ERROR_INVALID_ARGUMENT,
+                     "cola_batch_create_from_graphs: graph %d is NULL or has no row view", i);
+        COLA_REQUIRE(graphs[i]->device == b->device, COLA_ERROR_INVALID_ARGUMENT,
+                     "cola_batch_create_from_graphs: graph %d lives on device %d, current device is %d", i,
+                     graphs[i]->device, b->device);
+    }
+    try {
+        b->graphs.assign(graphs, graphs + ngraphs);
+    } catch (const std::bad_alloc &) {
+        return fail(COLA_ERROR_OUT_OF_MEMORY, "cola_batch_create_from_graphs: host allocation failed");
+    }
+    *out = b.release();
+    return COLA_SUCCESS;
+}
+
 cola_status cola_batch_free(cola_batch *b)
 {
     batch_release(b);

@@ -419,6 +419,34 @@ cola_status cola_server_register(cola_server *S, const cola_partition_set *parts
     return COLA_SUCCESS;
 }
 
+cola_status cola_server_register_graph(cola_server *S, cola_graph *g, int32_t *graph_id)
+{
+    if (!(S && g && graph_id)) {
+        graph_release(g);  // ownership was passed: never leak it
+        return fail(COLA_ERROR_INVALID_ARGUMENT, "cola_server_register_graph: null argument");
+    }
+    if (!g->has_rows || g->device != S->device) {
+        const int dev = g->device;
+        graph_release(g);
+        return fail(COLA_ERROR_INVALID_ARGUMENT,
+                    "cola_server_register_graph: the graph needs its row view and the server's device %d (it "
+                    "lives on %d)", S->device, dev);
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->used + (int64_t)g->dbytes > S->budget) {
+        const size_t need = g->dbytes;
+        graph_release(g);
+        return fail(COLA_ERROR_BUDGET, "cola_server_register_graph: graph needs %zu bytes, %lld of %lld bytes in use",
+                    need, (long long)S->used, (long long)S->budget);
+    }
+    S->used += (int64_t)g->dbytes;
+    S->graph_bytes += (int64_t)g->dbytes;
+    S->peak_used = std::max(S->peak_used, S->used);
+    S->graphs.push_back(g);
+    *graph_id = (int32_t)S->graphs.size() - 1;
+    return COLA_SUCCESS;
+}
+
 cola_status cola_server_submit(cola_server *S, int32_t graph_id, const void *X_host, cola_dtype x_dtype,
                                int32_t K, void *Y_host, cola_dtype y_dtype, uint64_t *request_id)
 {

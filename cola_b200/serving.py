@@ -57,6 +57,15 @@ class Server:
         self.num_nodes.append(pset.num_nodes)
         return gid.value
 
+    def register_graph(self, graph):
+        """Register an existing Graph (for example Graph.from_coo_device); the
+        server takes it over: the Graph object is empty afterwards."""
+        h, graph._h = graph._h, None
+        gid = ctypes.c_int32()
+        check(lib().cola_server_register_graph(self._h, h, ctypes.byref(gid)))
+        self.num_nodes.append(graph.num_nodes)
+        return gid.value
+
     def submit(self, graph_id, X, out_dtype=torch.float32, Y=None):
         """X: host tensor N x K (float32 or bfloat16; pinned memory lets copies
         overlap).  Returns a Request whose wait() gives Y (host, out_dtype)."""

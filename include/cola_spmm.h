@@ -372,6 +372,11 @@ typedef struct cola_batch cola_batch;
  * cola_graph_upload does); opts applies to all of them and may be NULL. */
 cola_status cola_batch_create(const cola_partition_set *const *parts, int32_t ngraphs, const cola_upload_opts *opts,
                               cola_batch **out, cola_stream_t stream);
+/* A batch over graphs that already exist (cola_graph_upload with the row
+ * view, or cola_graph_build_device).  The batch borrows them (free the batch
+ * first, then the graphs) and uses each graph's hub workspace, so a graph of
+ * the batch must not run elsewhere while the batch runs. */
+cola_status cola_batch_create_from_graphs(cola_graph *const *graphs, int32_t ngraphs, cola_batch **out);
 cola_status cola_batch_free(cola_batch *b);
 
 /* Bind graph g's dense operands: X[g] (>= N_g rows, ldx[g]), Y[g] (N_g rows,
@@ -439,6 +444,11 @@ cola_status cola_server_destroy(cola_server *s);
  * bytes count against the budget (COLA_ERROR_BUDGET if they do not fit). */
 cola_status cola_server_register(cola_server *s, const cola_partition_set *parts, const cola_upload_opts *opts,
                                  int32_t *graph_id);
+
+/* Register a graph that already exists (cola_graph_upload with the row view,
+ * or cola_graph_build_device).  The server takes ownership of g in every case
+ * (it is freed on failure and at cola_server_destroy). */
+cola_status cola_server_register_graph(cola_server *s, cola_graph *g, int32_t *graph_id);
 
 /* Queue Y = A_graph X.  X_host: N x K row-major host memory in x_dtype (pinned
  * memory lets the copies overlap); Y_host: N x K in y_dtype, written when the

@@ -136,3 +136,29 @@ def test_batch_rejects_bad_binding(graphs):
         b.bind([torch.zeros((1, 8), device=DEV)] * 2, [torch.zeros((1, 8), device=DEV)] * 2)
     with pytest.raises(cb.ColaError):
         b.run()  # nothing bound
+
+
+def test_batch_from_existing_graphs_device_built(graphs):
+    # graphs built on the device, batched without another upload: each result
+    # within the bound of FP64, and the same bits as the graph's own SpMM where
+    # both use full 32-lane row tiles (K >= 128 FP32); narrower rows are cut
+    # into lane groups of other widths by the two kernels (8 lanes minimum in
+    # the batched form), which changes the order of the float sums
+    from cola_b200 import spmm as S
+    gs = [S.Graph.from_coo_device(n, torch.from_numpy(row).to(DEV), torch.from_numpy(col).to(DEV),
+                                  torch.from_numpy(val).to(DEV), 4) for n, row, col, val, _ in graphs[:5]]
+    b = Batch.from_graphs(gs)
+    Ks = [16, 64, 128, 32, 256]
+    Xs = [torch.from_numpy(dense_x(g.num_nodes, K, seed=K)).to(DEV) for g, K in zip(gs, Ks)]
+    Ys = [torch.zeros((g.num_nodes, K), device=DEV) for g, K in zip(gs, Ks)]
+    b.bind(Xs, Ys)
+    b.run()
+    torch.cuda.synchronize()
+    for g, X, Y, (n, row, col, val, _) in zip(gs, Xs, Ys, graphs[:5]):
+        alone = g.spmm(X)
+        torch.cuda.synchronize()
+        if X.shape[1] >= 128:
+            assert torch.equal(Y, alone)
+        assert rel(Y.cpu().numpy(), fp64_reference(n, row, col, val, X.cpu().numpy())) <= TOL_F32
+    b.close()
+    del gs

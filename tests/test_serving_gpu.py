@@ -127,3 +127,23 @@ def test_bad_requests(graphs):
     with pytest.raises(ValueError):
         srv.submit(gid + 5, host_x(n, 16, seed=1))
     srv.close()
+
+
+def test_register_device_built_graph(graphs):
+    from cola_b200 import spmm as S
+    n, row, col, val, ps = graphs[0]
+    dev = [torch.from_numpy(a).cuda() for a in (row, col, val)]
+    srv = Server()
+    gid_dev = srv.register_graph(S.Graph.from_coo_device(n, *dev, ps.nparts))
+    gid_up = srv.register(ps)
+    X = host_x(n, 64, seed=5)
+    y_dev = srv.submit(gid_dev, X).wait()
+    y_up = srv.submit(gid_up, X).wait()
+    assert torch.equal(y_dev, y_up)  # same graph, same bits
+    assert rel(y_dev.numpy(), fp64_reference(n, row, col, val, X.numpy())) <= TOL_F32
+    # a graph without its row view is refused (and freed)
+    g = S.Graph(ps, row_view=False)
+    with pytest.raises(cb.ColaError):
+        srv.register_graph(g)
+    assert g.handle is None
+    srv.close()
