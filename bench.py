@@ -368,8 +368,9 @@ def run_ours(args, w):
         g.spmm(X, Yacc, accumulate=(eff == S.SCHEDULE_FUSED), schedule=sched, unroll=args.unroll, min_blocks=args.min_blocks, stream=stream)
         b.record(stream)
     torch.cuda.synchronize()
-    k_ms = sum(a.elapsed_time(b) for a, b in kev) / len(kev)
-    k_ms = max_over_ranks(k_ms)
+    k_list = [a.elapsed_time(b) for a, b in kev]
+    k_ms = max_over_ranks(sum(k_list) / len(k_list))
+    k_med = max_over_ranks(statistics.median(k_list))
     clk = clocks.stop()
     del Yacc
 
@@ -467,7 +468,11 @@ def run_ours(args, w):
                    "prep_seconds": round(t_prep, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
-                     "kernel_ms": k_ms, "frac_of_8TBs": achieved / 8000.0},
+                     "kernel_ms": k_ms, "kernel_ms_median": k_med, "frac_of_8TBs": achieved / 8000.0,
+                     # what must cross DRAM at least: indices and values once, X and Y once
+                     "compulsory_bytes": int(info.nnz) * 8 + n * K * (s_x + s_y),
+                     "traffic_over_compulsory": None if traffic is None else
+                     traffic / float(int(info.nnz) * 8 + n * K * (s_x + s_y))},
         "e2e": None if e2e_ms is None else {
             "value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": n * K * s_x,
             "d2h_bytes_per_step": n * K * s_y, "ms_per_step": e2e_ms,
@@ -482,7 +487,7 @@ def run_ours(args, w):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle
-        rp, ci, _ = oracle.global_csr(n, row, col, val)
+        rp, ci, vv = oracle.global_csr(n, row, col, val)
         nth = host_threads()
         dt, rows, nnz, kind, rows_per = calibrated_cpu(rp, ci, Xh, K, nth, target_s=2.0)
         reps = 3
@@ -495,6 +500,27 @@ def run_ours(args, w):
                                 "sample": "SAG_reference_host (include/utils.cuh:45-69) over {} threads x {} rows "
                                           "spread over the matrix ({} nnz), FP32 X, median of {}".format(
                                               nth, rows_per, nnz, reps)}
+        # beside it, torch.sparse.mm on the host over the whole global CSR (FP32)
+        try:
+            import warnings
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore")  # torch marks sparse CSR as beta
+                A = torch.sparse_csr_tensor(torch.from_numpy(rp.astype(np.int64)),
+                                            torch.from_numpy(ci.astype(np.int64)), torch.from_numpy(vv),
+                                            size=(n, n), check_invariants=False)
+            Xc = torch.from_numpy(Xh if Xh.dtype == np.float32 else Xh.astype(np.float32))
+            torch.set_num_threads(nth)
+            torch.sparse.mm(A, Xc[:, :8])
+            tt = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                torch.sparse.mm(A, Xc)
+                tt.append(time.perf_counter() - t0)
+            line["cpu_baseline"]["torch_sparse_mm"] = {
+                "value": alg_bytes(len(ci), n, K, 4, 4) / statistics.median(tt) / 1e9, "unit": "GB/s",
+                "cores": nth, "sample": "the whole matrix, FP32, median of 3"}
+        except (RuntimeError, MemoryError) as e:
+            line["cpu_baseline"]["torch_sparse_mm"] = {"unavailable": str(e)[:200]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.close()
