@@ -18,10 +18,12 @@
 // their positions are the row (column) pointers.  All of it is integer work
 // bound by HBM: the sort moves 12 bytes per entry per 8-bit digit.
 #include <algorithm>
+#include <array>
 #include <climits>
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -608,19 +610,26 @@ struct HostCopy {
 };
 
 static std::mutex g_stage_mu;
-static char *g_stage[2] = {nullptr, nullptr};
-static cudaEvent_t g_stage_ev[2] = {nullptr, nullptr};
+static char *g_stage[2] = {nullptr, nullptr};  // pinned: reachable from every device
+static std::unordered_map<int, std::array<cudaEvent_t, 2>> g_stage_ev;  // events belong to one device
 constexpr size_t kStageBytes = 16u << 20;
 
 static cola_status copy_to_host(const std::vector<HostCopy> &jobs, cudaStream_t st)
 {
     std::lock_guard<std::mutex> lk(g_stage_mu);
-    for (int b = 0; b < 2; b++) {
+    int dev = 0;
+    COLA_CUDA(cudaGetDevice(&dev));
+    for (int b = 0; b < 2; b++)
         if (!g_stage[b])
             COLA_CUDA(cudaMallocHost((void **)&g_stage[b], kStageBytes));
-        if (!g_stage_ev[b])
-            COLA_CUDA(cudaEventCreateWithFlags(&g_stage_ev[b], cudaEventDisableTiming));
+    auto it = g_stage_ev.find(dev);
+    if (it == g_stage_ev.end()) {
+        std::array<cudaEvent_t, 2> ev{};
+        for (cudaEvent_t &e : ev)
+            COLA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        it = g_stage_ev.emplace(dev, ev).first;
     }
+    const std::array<cudaEvent_t, 2> &stage_ev = it->second;
     // pieces of at most one chunk, packed into chunks in order
     struct Piece {
         char *dst;
@@ -647,7 +656,7 @@ static cola_status copy_to_host(const std::vector<HostCopy> &jobs, cudaStream_t 
         char *buf = g_stage[c & 1];
         for (const Piece &p : chunks[c])
             COLA_CUDA(cudaMemcpyAsync(buf + p.off, p.src, p.bytes, cudaMemcpyDeviceToHost, st));
-        COLA_CUDA(cudaEventRecord(g_stage_ev[c & 1], st));
+        COLA_CUDA(cudaEventRecord(stage_ev[c & 1], st));
         return COLA_SUCCESS;
     };
     if (chunks[0].empty())
@@ -656,7 +665,7 @@ static cola_status copy_to_host(const std::vector<HostCopy> &jobs, cudaStream_t 
     for (size_t c = 0; c < chunks.size(); c++) {
         if (c + 1 < chunks.size())
             COLA_TRY(issue(c + 1));  // the other buffer: its previous chunk was spread already
-        COLA_CUDA(cudaEventSynchronize(g_stage_ev[c & 1]));
+        COLA_CUDA(cudaEventSynchronize(stage_ev[c & 1]));
         const char *buf = g_stage[c & 1];
         const std::vector<Piece> &ps = chunks[c];
         // spread in 256 KiB slices over the host threads
