@@ -11,6 +11,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <system_error>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -322,11 +323,42 @@ using namespace cola;
 
 extern "C" {
 
+// Device resources of a server whose scheduler is not running (never started
+// or joined): streams after their work, descriptors, events, graphs, the
+// memory pool, leftover requests; then the server itself.
+static void server_release(cola_server *S)
+{
+    if (!S)
+        return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(S->device);
+    for (Slot &sl : S->slots) {
+        if (sl.stream) {
+            cudaStreamSynchronize(sl.stream);
+            cudaStreamDestroy(sl.stream);
+        }
+        cudaFree(sl.d_desc);
+        cudaFreeHost(sl.h_desc);
+        for (cudaEvent_t e : sl.ev)
+            if (e)
+                cudaEventDestroy(e);
+    }
+    for (cola_graph *g : S->graphs)
+        graph_release(g);
+    if (S->pool)
+        cudaMemPoolDestroy(S->pool);
+    for (auto &kv : S->reqs)
+        delete kv.second;
+    cudaSetDevice(cur);
+    delete S;
+}
+
 cola_status cola_server_create(const cola_server_opts *opts, cola_server **out)
 {
     COLA_REQUIRE(out, COLA_ERROR_INVALID_ARGUMENT, "cola_server_create: out is NULL");
     *out = nullptr;
-    std::unique_ptr<cola_server> S(new (std::nothrow) cola_server());
+    std::unique_ptr<cola_server, void (*)(cola_server *)> S(new (std::nothrow) cola_server(), server_release);
     COLA_REQUIRE(S, COLA_ERROR_OUT_OF_MEMORY, "cola_server_create: host allocation failed");
     COLA_CUDA(cudaGetDevice(&S->device));
     S->budget = opts && opts->memory_budget > 0 ? opts->memory_budget : (int64_t)120 << 30;
@@ -341,7 +373,11 @@ cola_status cola_server_create(const cola_server_opts *opts, cola_server **out)
     COLA_CUDA(cudaMemPoolCreate(&S->pool, &pp));
     uint64_t keep = (uint64_t)S->budget;
     COLA_CUDA(cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep));
-    S->slots.resize((size_t)nslots);
+    try {
+        S->slots.resize((size_t)nslots);
+    } catch (const std::bad_alloc &) {
+        return fail(COLA_ERROR_OUT_OF_MEMORY, "cola_server_create: host allocation failed");
+    }
     for (Slot &sl : S->slots) {
         COLA_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
         COLA_CUDA(cudaMalloc(&sl.d_desc, (size_t)S->max_group * sizeof(BatchGraph)));
@@ -350,7 +386,11 @@ cola_status cola_server_create(const cola_server_opts *opts, cola_server **out)
         for (cudaEvent_t &e : sl.ev)
             COLA_CUDA(cudaEventCreate(&e));
     }
-    S->th = std::thread(scheduler, S.get());
+    try {
+        S->th = std::thread(scheduler, S.get());
+    } catch (const std::system_error &) {
+        return fail(COLA_ERROR_OUT_OF_MEMORY, "cola_server_create: cannot start the scheduler thread");
+    }
     *out = S.release();
     return COLA_SUCCESS;
 }
@@ -370,26 +410,7 @@ cola_status cola_server_destroy(cola_server *S)
     }
     S->cv_sched.notify_all();
     S->th.join();  // returns once every admitted group has completed
-    int cur = 0;
-    cudaGetDevice(&cur);
-    cudaSetDevice(S->device);
-    for (Slot &sl : S->slots) {
-        cudaStreamSynchronize(sl.stream);
-        cudaStreamDestroy(sl.stream);
-        cudaFree(sl.d_desc);
-        cudaFreeHost(sl.h_desc);
-        for (cudaEvent_t e : sl.ev)
-            if (e)
-                cudaEventDestroy(e);
-    }
-    for (cola_graph *g : S->graphs)
-        graph_release(g);
-    if (S->pool)
-        cudaMemPoolDestroy(S->pool);
-    for (auto &kv : S->reqs)
-        delete kv.second;
-    cudaSetDevice(cur);
-    delete S;
+    server_release(S);
     return COLA_SUCCESS;
 }
 
