@@ -23,6 +23,8 @@
 
 #include <cuda_runtime_api.h>
 
+#include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
@@ -306,6 +308,112 @@ inline void distSpMM_ppl_batch_all(const int group_size, float *output, const fl
                                      remote_offset_ppl[me][2 * i + 1], i, idx_ppl[me][i - 1], dim, nodesPerPE,
                                      group_size, me / group_size * group_size, me, stream);
     }
+}
+
+/* include/utils.cuh:45-69: the unweighted host reference of rows [lb, ub):
+ * C_ref[i, :] = sum over the row's stored columns k of B[k, :] (values are not
+ * read; the reference's are all 1). */
+template <typename Index, typename DType>
+void SAG_reference_host(int lb, int ub, int N, const Index *csr_indptr, const int *csr_indices, const DType *B,
+                        DType *C_ref, int peid)
+{
+    (void)peid;
+    const int64_t M = ub > lb ? ub - lb : 0;
+    for (int64_t x = 0; x < M * (int64_t)N; x++)
+        C_ref[x] = DType(0);
+    for (int64_t i = 0; i < M; i++) {
+        DType *c = C_ref + i * N;
+        for (Index p = csr_indptr[lb + i]; p < csr_indptr[lb + i + 1]; p++) {
+            const DType *b = B + (int64_t)csr_indices[p] * N;
+            for (int64_t j = 0; j < N; j++)
+                c[j] += b[j];
+        }
+    }
+}
+
+/* include/utils.cuh:71-101: element-wise check with relative tolerance 1e-2.
+ * Prints the first 33 mismatches as the reference does; returns whether all
+ * elements passed (the reference exits the process after 33 mismatches). */
+template <typename DType>
+bool check_result(int M, int N, const DType *C, const DType *C_ref, int PEid)
+{
+    int64_t bad = 0;
+    for (int64_t i = 0; i < M; i++)
+        for (int64_t j = 0; j < N; j++) {
+            const double c = (double)C[i * N + j], r = (double)C_ref[i * N + j];
+            if (!(std::fabs(c - r) <= 1e-2 * std::fabs(r))) {
+                if (bad <= 32)
+                    printf("peid-%d Wrong result: i = %lld, j = %lld, result = %lf, reference = %lf.\n", PEid,
+                           (long long)i, (long long)j, c, r);
+                bad++;
+            }
+        }
+    if (bad == 0)
+        printf("PEid-%d passed\n", PEid);
+    return bad == 0;
+}
+
+/* include/dist_spmm_ppl_batch.cuh:920-987 for one virtual PE: one SpMM into
+ * `output` (accumulated, as the reference's kernels do), then optionally a
+ * validation of rows [block_lb, block_ub) against SAG_reference_host over the
+ * global CSR with host features h_in (the caller zeroes output first, as the
+ * reference's main does), then optionally 200 timed SpMMs after warm-up,
+ * timed with CUDA events on `stream` (the reference: MPI_Wtime between
+ * barriers).  Returns the average milliseconds per SpMM when profiling, else
+ * 0; throws cola_compat::error when validation fails. */
+template <bool validate, bool profiling, bool profile_detail = false>
+double run_distSpMM_ppl_batch(const int group_size, float *output, const float *input_nvsh, float **ppl_buffer_nvsh,
+                              float *ppl_send_nvsh, float *comm_buffer_nvsh, int *local_offset_ppl,
+                              int *remote_offset_ppl, int *put_offset_ppl, int **put_colIdx_ppl, int **idx_ppl,
+                              d_csr_zip *csr_zip_l, d_csc_zip *csc_zip_r, const int block_lb, const int block_ub,
+                              const int dim, const int nodesPerPE, const int nranks, const int mype_node,
+                              const int *global_rowPtr, const int *global_colIdx, const float *h_in,
+                              cudaStream_t stream)
+{
+    if (mype_node == 0 && (validate || profiling))
+        printf("Running ppl_batch SpMM with group_size:%d\n", group_size);
+    auto once = [&]() {
+        distSpMM_ppl_batch_wrapper(group_size, output, input_nvsh, ppl_buffer_nvsh, ppl_send_nvsh, comm_buffer_nvsh,
+                                   local_offset_ppl, remote_offset_ppl, put_offset_ppl, put_colIdx_ppl, idx_ppl,
+                                   csr_zip_l, csc_zip_r, block_lb, block_ub, dim, nodesPerPE, nranks, mype_node,
+                                   stream);
+    };
+    once();
+    cola_compat::check_cuda(cudaStreamSynchronize(stream), "run_distSpMM_ppl_batch");
+    if (validate) {
+        const int M = block_ub - block_lb;
+        std::vector<float> out((size_t)M * dim), ref((size_t)M * dim);
+        SAG_reference_host<int, float>(block_lb, block_ub, dim, global_rowPtr, global_colIdx, h_in, ref.data(),
+                                       mype_node);
+        cola_compat::check_cuda(cudaMemcpy(out.data(), output, out.size() * sizeof(float), cudaMemcpyDeviceToHost),
+                                "run_distSpMM_ppl_batch");
+        if (!check_result(M, dim, out.data(), ref.data(), mype_node))
+            throw cola_compat::error(COLA_ERROR_INVALID_ARGUMENT, "run_distSpMM_ppl_batch: validation failed");
+    }
+    double ms = 0.0;
+    if (profiling) {
+        const int num_profiling = 200;
+        for (int i = 0; i < 50; i++)
+            once();
+        cudaEvent_t e0, e1;
+        cola_compat::check_cuda(cudaEventCreate(&e0), "run_distSpMM_ppl_batch");
+        cola_compat::check_cuda(cudaEventCreate(&e1), "run_distSpMM_ppl_batch");
+        cola_compat::check_cuda(cudaEventRecord(e0, stream), "run_distSpMM_ppl_batch");
+        for (int i = 0; i < num_profiling; i++)
+            once();
+        cola_compat::check_cuda(cudaEventRecord(e1, stream), "run_distSpMM_ppl_batch");
+        cola_compat::check_cuda(cudaEventSynchronize(e1), "run_distSpMM_ppl_batch");
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        ms = (double)t / num_profiling;
+        if (mype_node == 0) {
+            printf("nodesPerPE:%d\n", nodesPerPE);
+            printf("PE-%d time (ms) %.3f\n", mype_node, ms);
+        }
+    }
+    return ms;
 }
 
 #endif /* COLA_COMPAT_H */
