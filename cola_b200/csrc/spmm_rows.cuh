@@ -32,7 +32,7 @@ __device__ __forceinline__ void store_out<float, 4, true>(float *p, const float 
         v.z += o.z;
         v.w += o.w;
     }
-    *reinterpret_cast<float4 *>(p) = v;
+    __stcs(reinterpret_cast<float4 *>(p), v);  // Y is written once: evict-first in L2, X rows stay
 }
 
 template <>
@@ -53,8 +53,8 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
 template <>
 __device__ __forceinline__ void store_out<__nv_bfloat16, 8, true>(__nv_bfloat16 *p, const float (&a)[8], bool)
 {
-    *reinterpret_cast<uint4 *>(p) =
-        make_uint4(pack_bf16x2(a[0], a[1]), pack_bf16x2(a[2], a[3]), pack_bf16x2(a[4], a[5]), pack_bf16x2(a[6], a[7]));
+    __stcs(reinterpret_cast<uint4 *>(p),
+           make_uint4(pack_bf16x2(a[0], a[1]), pack_bf16x2(a[2], a[3]), pack_bf16x2(a[4], a[5]), pack_bf16x2(a[6], a[7])));
 }
 
 template <>
@@ -365,8 +365,9 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
         int mc = 0;
         float mv = 0.f;
         if (lane < n_ent) {
-            mc = __ldg(colp + lane);
-            mv = __ldg(valp + lane);
+            // the entry stream is read once: evict-first, so it does not push X rows out of L2
+            mc = __ldcs(colp + lane);
+            mv = __ldcs(valp + lane);
         }
         for (int32_t base = 0; base < n_ent; base += 32) {
             const int n = min(32, n_ent - base);
@@ -375,8 +376,8 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
             __syncwarp();
             // prefetch the next index batch while this one is consumed
             if (base + 32 + lane < n_ent) {
-                mc = __ldg(colp + base + 32 + lane);
-                mv = __ldg(valp + base + 32 + lane);
+                mc = __ldcs(colp + base + 32 + lane);
+                mv = __ldcs(valp + base + 32 + lane);
             }
             for (int jj = 0; jj < n; jj += R) {
                 raw_t xr[UNROLL][NV];
