@@ -221,3 +221,41 @@ def test_device_graph_is_rows_only_and_edge_cases():
     assert torch.all(y0 == 0) and torch.all(y1 == 7.5)
     with pytest.raises(cb.ColaError, match="entry 1"):
         device_graph(4, np.array([0, 4], np.int32), np.array([1, 1], np.int32), None, 2)
+
+
+try:
+    from hypothesis import HealthCheck, given, settings
+    from hypothesis import strategies as st
+
+    @st.composite
+    def small_coo(draw):
+        n = draw(st.integers(1, 60))
+        nnz = draw(st.integers(0, 300))
+        row = np.array(draw(st.lists(st.integers(0, n - 1), min_size=nnz, max_size=nnz)), np.int32)
+        col = np.array(draw(st.lists(st.integers(0, n - 1), min_size=nnz, max_size=nnz)), np.int32)
+        val = np.array(draw(st.lists(st.floats(-4, 4, width=32), min_size=nnz, max_size=nnz)), np.float32)
+        P = draw(st.integers(1, 9))
+        thr = draw(st.sampled_from([0, 1, 3, 8]))
+        seg = draw(st.sampled_from([0, 1, 2, 5]))
+        te = draw(st.sampled_from([0, 1, 4, 16]))
+        return n, row, col, val, P, thr, seg, te
+
+    @settings(max_examples=60, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+    @given(small_coo())
+    def test_device_builds_match_host_on_random_coo(case):
+        n, row, col, val, P, thr, seg, te = case
+        assert_same_sets(build_device(n, row, col, val, P), cb.PartitionSet.from_coo(n, row, col, val, P), P,
+                         "random")
+        kw = dict(hub_threshold=thr, hub_segment=seg, task_entries=te)
+        gd = device_graph(n, row, col, val, P, **kw)
+        gh = S.Graph(cb.PartitionSet.from_coo(n, row, col, val, P), **kw)
+        for k in ("nnz", "nnz_local", "hub_rows", "hub_segments", "row_tasks"):
+            assert getattr(gd.info, k) == getattr(gh.info, k), k
+        for K in (4, 64):
+            X = torch.from_numpy(dense_x(n, K, seed=K)).to(DEV)
+            a = gd.spmm(X)
+            b = gh.spmm(X, schedule=S.SCHEDULE_ROWS)
+            torch.cuda.synchronize()
+            assert torch.equal(a, b)
+except ImportError:  # hypothesis is optional for the GPU run
+    pass
