@@ -525,12 +525,88 @@ def run_ours(args, w):
                 "cores": nth, "sample": "the whole matrix, FP32, median of 3"}
         except (RuntimeError, MemoryError) as e:
             line["cpu_baseline"]["torch_sparse_mm"] = {"unavailable": str(e)[:200]}
+        # and an OpenMP loop over the same P partitions (local CSR + remote CSC chunks)
+        line["cpu_baseline"]["openmp_partitions"] = openmp_partitions_baseline(ps, Xh, K, w["P"], nth)
+        # the reference's own CUDA kernels on this GPU (FP32 only, as the reference)
+        if xdt == torch.float32 and ydt == torch.float32:
+            line["reference_gpu_kernels"] = reference_kernels_baseline(g, X, n, K, w["P"], B, k_ms, stream)
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def openmp_partitions_baseline(ps, Xh, K, P, nthreads):
+    """The oracle's OpenMP FP32 loop over the P partitions (their split local
+    CSR and remote CSC chunks, one thread per partition), whole matrix, median
+    of 3."""
+    from oracle import oracle
+    parts = [ps.part(r) for r in range(P)]
+    run = oracle.partitions_f32_omp(parts, ps.nodes_per_part, Xh)
+    nt = min(P, nthreads)
+    run(nt)
+    tt = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        run(nt)
+        tt.append(time.perf_counter() - t0)
+    nnz = sum(len(p["csr_colIdx_l"]) + len(p["csc_rowIdx_r"]) for p in parts)
+    return {"value": alg_bytes(nnz, Xh.shape[0], K, 4, 4) / statistics.median(tt) / 1e9, "unit": "GB/s",
+            "cores": nt, "sample": "the whole matrix, FP32, one OpenMP thread per partition (the oracle's "
+                                   "orc_spmm_partitions_f32_omp), median of 3"}
+
+
+def reference_kernels_baseline(g, X, n, K, P, B, k_ms, stream, steps=10):
+    """The reference's own ppl0_batch_SpMM<ceil(K/32), K%32 != 0> (compiled for
+    sm_100a through the NVSHMEM shim), launched once per virtual partition on
+    this graph's split blocks; the sum of the P kernel durations (CUDA events)
+    per SpMM, averaged over `steps` SpMMs after warm-up."""
+    import ctypes
+
+    import torch
+    from oracle import oracle
+    if not oracle.ref_available():
+        return {"unavailable": "the reference's kernels are not built (oracle/_ref)"}
+    R = oracle.ref()
+    CF, res = (K + 31) // 32, 1 if K & 31 else 0
+    if CF not in (1, 2, 3, 4, 8, 16):
+        return {"unavailable": "no reference instantiation for K={}".format(K)}
+    npp = g.nodes_per_part
+    Xr = torch.zeros((P * npp, K), device=X.device)
+    Xr[:n] = X.float()
+    Yr = torch.zeros((P * npp, K), device=X.device)
+    zips = [g.zip_view(p) for p in range(P)]
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(P)]
+
+    def spmm():
+        total = 0.0
+        for p, z in enumerate(zips):
+            if R.ref_set_pe(p, npp * K, sh) != 0:
+                raise RuntimeError("ref_set_pe failed")
+            a, b = evs[p]
+            a.record(stream)
+            rc = R.ref_ppl0_batch_spmm(CF, res, ctypes.c_void_p(Yr[p * npp:].data_ptr()),
+                                       ctypes.c_void_p(Xr[p * npp:].data_ptr()), z.csr_rowPtr, z.csr_colIdx,
+                                       z.csr_rowIdx_zip, z.csr_val, z.csc_colPtr, z.csc_rowIdx, z.csc_colIdx_zip,
+                                       z.csc_val, 0, 0, z.local_chunks, z.remote_chunks, K, npp, p, sh)
+            b.record(stream)
+            if rc != 0:
+                raise RuntimeError("reference kernel launch failed")
+        torch.cuda.synchronize()
+        for a, b in evs:
+            total += a.elapsed_time(b)
+        return total
+    for _ in range(3):
+        spmm()
+    ms = sum(spmm() for _ in range(steps)) / steps
+    del Xr, Yr
+    return {"ms_per_spmm": ms, "value": B / (ms * 1e-3) / 1e9, "unit": "GB/s",
+            "kernel": "ppl0_batch_SpMM<{}, {}> per virtual partition (include/dist_spmm_ppl_batch.cuh:76-245), "
+                      "sum of the {} kernel durations".format(CF, "true" if res else "false", P),
+            "ours_speedup": ms / k_ms}
 
 
 def make_batched(count, seed):

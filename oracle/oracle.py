@@ -43,7 +43,7 @@ def lib():
         L.orc_spmm_csr_f64.argtypes = [I64, P, P, P, P, I64, I32, P, I64]
         L.orc_spmm_csr_f64_bf16x.argtypes = [I64, P, P, P, P, I64, I32, P, I64]
         L.orc_spmm_partition_f64.argtypes = [I32, I32, P, P, P, P, I64, P, P, P, P, I64, P, I64, I32, P, I64]
-        L.orc_spmm_partitions_f32_omp.argtypes = [I32, I32] + [P] * 16 + [I64, I32, P, I64, I32]
+        L.orc_spmm_partitions_f32_omp.argtypes = [I32, I32] + [P] * 15 + [I64, I32, P, I64, I32]
         L.orc_max_threads.restype = I32
         _lib = L
     return _lib
@@ -230,6 +230,43 @@ def spmm_partition_f64(part, npp, lz, rz, X):
                              _ptr(rz[0]), _ptr(rz[1]), _ptr(rz[2]), _ptr(rz[3]), len(rz[2]),
                              _ptr(X), X.shape[1], K, _ptr(Y), K)
     return Y
+
+
+def partitions_f32_omp(parts, npp, X):
+    """The OpenMP FP32 loop over the partitions (orc_spmm_partitions_f32_omp:
+    each partition's split local CSR chunks and remote CSC chunks, as
+    nnz_split makes them, one thread per partition).  parts: the partition
+    dicts (csr_* / csc_* arrays with values).  Returns run(nthreads) -> Y
+    ((P * npp) x K, FP32); the arrays are prepared once."""
+    L = lib()
+    P = len(parts)
+    K = X.shape[1]
+    cols = {k: [] for k in ("l_ptr", "l_col", "l_val", "l_row", "r_ptr", "r_row", "r_val", "r_col")}
+    for p in parts:
+        lt, lq = nnz_split(p["csr_rowIdx_l"], p["csr_rowPtr_l"], len(p["csr_colIdx_l"]))
+        rt, rq = nnz_split(p["csc_colIdx_r"], p["csc_colPtr_r"], len(p["csc_rowIdx_r"]))
+        z = np.zeros(1, np.int32)
+        for k, a in (("l_ptr", lq if len(lq) else z), ("l_col", p["csr_colIdx_l"]), ("l_val", p["csr_val_l"]),
+                     ("l_row", lt), ("r_ptr", rq if len(rq) else z), ("r_row", p["csc_rowIdx_r"]),
+                     ("r_val", p["csc_val_r"]), ("r_col", rt)):
+            cols[k].append(np.ascontiguousarray(a))
+    arr = {}
+    for k, v in cols.items():
+        dt = np.float32 if k.endswith("val") else np.int32
+        arr[k] = (np.ascontiguousarray(np.concatenate(v).astype(dt)),
+                  np.concatenate([[0], np.cumsum([len(x) for x in v])]).astype(np.int64))
+    Xp = np.zeros((P * npp, K), np.float32)
+    Xp[:X.shape[0]] = X
+    Y = np.empty((P * npp, K), np.float32)
+
+    def run(nthreads):
+        L.orc_spmm_partitions_f32_omp(
+            P, npp, _ptr(arr["l_ptr"][0]), _ptr(arr["l_ptr"][1]), _ptr(arr["l_col"][0]), _ptr(arr["l_val"][0]),
+            _ptr(arr["l_col"][1]), _ptr(arr["l_row"][0]), _ptr(arr["l_row"][1]), _ptr(arr["r_ptr"][0]),
+            _ptr(arr["r_ptr"][1]), _ptr(arr["r_row"][0]), _ptr(arr["r_val"][0]), _ptr(arr["r_row"][1]),
+            _ptr(arr["r_col"][0]), _ptr(arr["r_col"][1]), _ptr(Xp), K, K, _ptr(Y), K, int(nthreads))
+        return Y
+    return run
 
 
 def rel_frobenius(y, ref):
