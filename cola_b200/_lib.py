@@ -100,6 +100,8 @@ SIGNATURES = {
     "cola_partition_get": (I32, [P, I32, P]),
     "cola_nnz_split": (I32, [P, I64, P, I64, P, P, I64, P]),
     "cola_partition_build_device": (I32, [I32, I64, P, P, P, I32, P, P]),
+    "cola_set_gather_bulk": (I32, [I32]),
+    "cola_device_error_check": (I32, [P]),
     "cola_graph_build_device": (I32, [I32, I64, P, P, P, I32, P, P, P]),
     "cola_nnz_split_device": (I32, [P, I64, P, I64, P, P, I64, P, P]),
     "cola_relabel_edges": (I32, [I32, I64, P, P, P, P, P]),

@@ -1,6 +1,7 @@
 // Launchers, kernel-level C ABI and the device-resident graph of the
 // partitioned SpMM (sm_100a).
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -151,12 +152,90 @@ static bool vec_ok(cola_dtype xdt, const void *X, int64_t ldx, const void *stage
 // ---------------------------------------------------------------------------
 // gather dispatch
 // ---------------------------------------------------------------------------
+// Set by a kernel whose bounded wait ran out (read and cleared by
+// cola_device_error_check); one per device.
+__device__ int g_dev_error = 0;
+
+static int *device_error_flag()
+{
+    static std::mutex mu;
+    static std::unordered_map<int, int *> by_dev;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = by_dev.find(dev);
+    if (it != by_dev.end())
+        return it->second;
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_dev_error) != cudaSuccess)
+        return nullptr;
+    by_dev[dev] = static_cast<int *>(p);
+    return static_cast<int *>(p);
+}
+
+static std::atomic<int> g_gather_bulk{1};
+
+// Bulk-copy (TMA) gather when every row and address is 16-byte aligned and at
+// least two row slots fit a warp's share of shared memory; returns false to
+// leave the rows to the vector gather.
+template <typename T>
+static bool launch_gather_bulk(const GatherSeg *segs, const GatherSeg &single, int nsegs, int64_t total,
+                               const void *src, int64_t ld_src, void *dst, int64_t ld_dst, int K, cudaStream_t st,
+                               cola_status &rc)
+{
+    const int64_t bytes = (int64_t)K * (int64_t)sizeof(T);
+    if (!g_gather_bulk.load() || bytes % 16 || (ld_src * (int64_t)sizeof(T)) % 16 ||
+        (ld_dst * (int64_t)sizeof(T)) % 16 || !aligned16(src) || !aligned16(dst))
+        return false;
+    constexpr int kBudget = 200 * 1024;  // dynamic shared memory per block (one block per SM)
+    const int slot = (int)((bytes + 127) / 128 * 128);
+    const int ns = (int)std::min<int64_t>(dev::kGatherMaxSlots, kBudget / dev::kWarpsPerBlock / std::max(slot, 1));
+    if (ns < 2)
+        return false;
+    int *err = device_error_flag();
+    if (!err)
+        return false;
+    auto fn = dev::gather_rows_bulk_kernel<T>;
+    const size_t smem = (size_t)dev::kWarpsPerBlock * ns * (slot + 8);
+    {
+        static std::mutex mu;
+        static std::unordered_map<int, size_t> set_for;  // per device: largest dynamic size allowed so far
+        int d = 0;
+        cudaGetDevice(&d);
+        std::lock_guard<std::mutex> lk(mu);
+        size_t &have = set_for[d * 2 + (sizeof(T) == 4 ? 0 : 1)];
+        if (have < smem) {
+            if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                cudaSuccess)
+                return false;
+            have = smem;
+        }
+    }
+    const int64_t need = (total + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock;
+    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>(need, sm_count()));
+    t_launches++;
+    fn<<<(unsigned)gx, dev::kThreads, smem, st>>>(segs, single, nsegs, total, static_cast<const T *>(src), ld_src,
+                                                  static_cast<T *>(dst), ld_dst, K, ns, slot, err);
+    const cudaError_t e = cudaGetLastError();
+    rc = e == cudaSuccess ? COLA_SUCCESS : fail(COLA_ERROR_CUDA, "gather (bulk copies): %s", cudaGetErrorString(e));
+    return true;
+}
+
 static cola_status launch_gather(const GatherSeg *segs, const GatherSeg &single, int nsegs, int64_t total,
                                  const void *src, int64_t ld_src, void *dst, int64_t ld_dst, int K, cola_dtype dt,
                                  cudaStream_t st)
 {
     if (total <= 0 || K <= 0)
         return COLA_SUCCESS;
+    {
+        cola_status rc = COLA_SUCCESS;
+        if (dt == COLA_FLOAT32 ? launch_gather_bulk<float>(segs, single, nsegs, total, src, ld_src, dst, ld_dst, K,
+                                                           st, rc)
+                               : launch_gather_bulk<__nv_bfloat16>(segs, single, nsegs, total, src, ld_src, dst,
+                                                                   ld_dst, K, st, rc))
+            return rc;
+    }
     const int E = dt == COLA_FLOAT32 ? 4 : 8;
     const bool vec = K % E == 0 && ld_src % E == 0 && ld_dst % E == 0 && aligned16(src) && aligned16(dst);
 #define COLA_GATHER(TR)                                                                                        \
@@ -980,6 +1059,27 @@ cola_status cola_graph_get_info(const cola_graph *g, cola_graph_info *o)
     o->hub_segments = g->nseg;
     o->row_tasks = g->ntask;
     o->last_launches = g->last_launches;
+    return COLA_SUCCESS;
+}
+
+cola_status cola_device_error_check(int32_t *code)
+{
+    COLA_REQUIRE(code, COLA_ERROR_INVALID_ARGUMENT, "cola_device_error_check: code is NULL");
+    *code = 0;
+    COLA_CUDA(cudaDeviceSynchronize());
+    int v = 0;
+    COLA_CUDA(cudaMemcpyFromSymbol(&v, g_dev_error, sizeof(int)));
+    if (v) {
+        const int zero = 0;
+        COLA_CUDA(cudaMemcpyToSymbol(g_dev_error, &zero, sizeof(int)));
+    }
+    *code = v;
+    return COLA_SUCCESS;
+}
+
+cola_status cola_set_gather_bulk(int32_t enable)
+{
+    g_gather_bulk.store(enable ? 1 : 0);
     return COLA_SUCCESS;
 }
 

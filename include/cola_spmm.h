@@ -321,6 +321,16 @@ typedef struct cola_graph_info {
 } cola_graph_info;
 cola_status cola_graph_get_info(const cola_graph *g, cola_graph_info *out);
 
+/* Staged row gathers (BUFFER staging, PIPELINE puts, cola_batching_data_ppl)
+ * move rows with bulk asynchronous copies through shared memory when every
+ * row and address is 16-byte aligned (enable = 1, the default), else with
+ * 16-byte vector loads and stores (enable = 0 forces that; same results). */
+cola_status cola_set_gather_bulk(int32_t enable);
+
+/* Waits for the current device, then reports (and clears) the error code a
+ * kernel left when one of its bounded waits ran out: 0 = none. */
+cola_status cola_device_error_check(int32_t *code);
+
 /* Device pointers of partition `part`'s split arrays (the d_csr_zip / d_csc_zip
  * members of include/sparse_data.h:28-77) and its chunk counts. */
 typedef struct cola_zip_view {

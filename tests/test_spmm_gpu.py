@@ -436,3 +436,65 @@ def test_rows_hub_combine_tiles_and_repeats(case12, K, thr, seg):
     for y in outs:
         assert rel(y.cpu().numpy(), ref) <= TOL_F32
     assert torch.equal(outs[0], outs[1]) and torch.equal(outs[1], outs[2])
+
+
+# ---------------------------------------------------------------------------
+# staged gathers by bulk asynchronous copies (TMA) vs 16-byte vectors
+# ---------------------------------------------------------------------------
+def _device_error():
+    code = ctypes.c_int32(-1)
+    assert cb.lib().cola_device_error_check(ctypes.byref(code)) == 0
+    return code.value
+
+
+@pytest.mark.parametrize("K", [4, 8, 96, 128, 1000, 4096, 3])
+def test_bulk_gather_copies_rows_exactly(K):
+    """The staged gather send[b] = X[idx[b] % npp] through bulk copies (rows of
+    16 B .. 4 KB; 3 columns and 16 KB rows fall back to vectors) gives exactly
+    the rows the vector gather and a plain index copy give, on repeated
+    calls, and no bounded wait runs out."""
+    npp, P, nemb = 700, 4, 2500
+    X = torch.from_numpy(dense_x(P * npp, K, seed=K)).to(DEV)
+    rng = np.random.Generator(np.random.Philox(K))
+    idx = torch.from_numpy(rng.integers(0, P * npp, nemb).astype(np.int32)).to(DEV)
+    want = X[(idx.long() % npp)]
+    outs = []
+    try:
+        for bulk in (1, 0, 1):
+            assert cb.lib().cola_set_gather_bulk(bulk) == 0
+            out = torch.full((nemb, K), float("nan"), device=DEV)
+            cb._lib.check(cb.lib().cola_batching_data_ppl(ptr(X), ptr(out), ptr(idx), nemb, K, npp, 1, None))
+            torch.cuda.synchronize()
+            outs.append(out)
+    finally:
+        cb.lib().cola_set_gather_bulk(1)
+    for o in outs:
+        assert torch.equal(o, want)
+    assert _device_error() == 0
+
+
+@pytest.mark.parametrize("K,xdt", [(4, torch.float32), (128, torch.float32), (256, torch.bfloat16),
+                                   (1000, torch.float32), (4096, torch.float32), (3, torch.float32)])
+def test_bulk_gather_schedules(case12, K, xdt):
+    """BUFFER staging and PIPELINE puts through bulk copies against the vector
+    gather (their float atomics sum in varying order, so within 1e-6) and the
+    FP64 oracle, and no bounded wait runs out."""
+    n, row, col, val, ps = case12
+    X = torch.from_numpy(dense_x(n, K, seed=K)).to(DEV).to(xdt)
+    outs = {}
+    try:
+        for bulk in (1, 0):
+            assert cb.lib().cola_set_gather_bulk(bulk) == 0
+            g = S.Graph(ps)
+            gp = S.Graph(ps, group_size=2)
+            outs[bulk] = (g.spmm(X, schedule=S.SCHEDULE_BUFFER, gather_batch_rows=300),
+                          gp.spmm(X, schedule=S.SCHEDULE_PIPELINE))
+            torch.cuda.synchronize()
+    finally:
+        cb.lib().cola_set_gather_bulk(1)
+    for j in range(2):
+        assert rel(outs[1][j].cpu().numpy(), outs[0][j].cpu().numpy()) <= 1e-6
+    assert _device_error() == 0
+    ref = fp64_reference(n, row, col, val, X.float().cpu().numpy())
+    assert rel(outs[1][0].cpu().numpy(), ref) <= TOL_F32
+    assert rel(outs[1][1].cpu().numpy(), ref) <= TOL_F32
