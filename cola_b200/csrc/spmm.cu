@@ -174,18 +174,20 @@ static int *device_error_flag()
     return static_cast<int *>(p);
 }
 
-static std::atomic<int> g_gather_bulk{1};
+static std::atomic<int> g_gather_bulk{0};  // off: the vector gather measured as fast or faster
 
-// Bulk-copy (TMA) gather when every row and address is 16-byte aligned and at
-// least two row slots fit a warp's share of shared memory; returns false to
-// leave the rows to the vector gather.
+// Bulk-copy (TMA) gather, when switched on, for rows of 1 KB or more (measured
+// alone: within 1 % of the vector gather from 1 KB to 4 KB, behind below 1 KB;
+// inside the BUFFER schedule's 4,096-row batches 2-7 % behind) when every row and
+// address is 16-byte aligned and at least two row slots fit a warp's share of
+// shared memory; returns false to leave the rows to the vector gather.
 template <typename T>
 static bool launch_gather_bulk(const GatherSeg *segs, const GatherSeg &single, int nsegs, int64_t total,
                                const void *src, int64_t ld_src, void *dst, int64_t ld_dst, int K, cudaStream_t st,
                                cola_status &rc)
 {
     const int64_t bytes = (int64_t)K * (int64_t)sizeof(T);
-    if (!g_gather_bulk.load() || bytes % 16 || (ld_src * (int64_t)sizeof(T)) % 16 ||
+    if (!g_gather_bulk.load() || bytes < 1024 || bytes % 16 || (ld_src * (int64_t)sizeof(T)) % 16 ||
         (ld_dst * (int64_t)sizeof(T)) % 16 || !aligned16(src) || !aligned16(dst))
         return false;
     constexpr int kBudget = 200 * 1024;  // dynamic shared memory per block (one block per SM)
@@ -214,9 +216,12 @@ static bool launch_gather_bulk(const GatherSeg *segs, const GatherSeg &single, i
     }
     const int64_t need = (total + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock;
     const int64_t gx = std::max<int64_t>(1, std::min<int64_t>(need, sm_count()));
+    // rows per chunk: all ns slots when there are rows enough for every warp
+    const int64_t per_warp = (total + gx * dev::kWarpsPerBlock - 1) / (gx * dev::kWarpsPerBlock);
+    const int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(ns, per_warp));
     t_launches++;
     fn<<<(unsigned)gx, dev::kThreads, smem, st>>>(segs, single, nsegs, total, static_cast<const T *>(src), ld_src,
-                                                  static_cast<T *>(dst), ld_dst, K, ns, slot, err);
+                                                  static_cast<T *>(dst), ld_dst, K, ns, chunk, slot, err);
     const cudaError_t e = cudaGetLastError();
     rc = e == cudaSuccess ? COLA_SUCCESS : fail(COLA_ERROR_CUDA, "gather (bulk copies): %s", cudaGetErrorString(e));
     return true;

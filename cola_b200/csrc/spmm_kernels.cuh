@@ -300,12 +300,14 @@ struct GatherSeg {
 // ---------------------------------------------------------------------------
 // Staged row gather through the Tensor Memory Accelerator: each row moves
 // global -> shared -> global with bulk asynchronous copies (cp.async.bulk of
-// one CTA, no tensor map), so no register or lane touches the data.  One
-// elected lane per warp drives a ring of `ns` shared-memory row slots (as many
-// as fit its share of the block's dynamic shared memory, at most 32): row k's
-// load completes on its slot's mbarrier, its store is issued as a bulk group,
-// and the slot of row k-1 is refilled with row k-1+ns once that row's store
-// has finished reading it.  Rows are K elements of 16-byte granularity, every
+// one CTA, no tensor map), so no register touches the row data.  A warp takes
+// chunks of `chunk` consecutive rows (at most its ns row slots of the block's
+// dynamic shared memory, at most 32; fewer when a launch has few rows, so that
+// every warp gets some): the lanes resolve the chunk's source and
+// destination rows together (one coalesced index load), then one elected lane
+// issues every row's load at once, stores each row as its load lands on the
+// slot's mbarrier, and waits for the stores to finish reading before the next
+// chunk reuses the slots.  Rows are K elements of 16-byte granularity, every
 // address 16-byte aligned (checked by the host).  Every wait is bounded: past
 // the limit the kernel records an error in *err, drains its own copies (again
 // bounded) and stops.
@@ -331,7 +333,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
 }
 
 // Source and destination row of gather item `it`; sidx walks the segments
-// forward (items are visited in increasing order).
+// forward (each lane visits its items in increasing order).
 template <typename T>
 __device__ __forceinline__ void gather_row(const GatherSeg *segs, const GatherSeg &single, int nsegs, int &sidx,
                                            int64_t it, const T *src, int64_t ld_src, T *dst, int64_t ld_dst,
@@ -359,71 +361,75 @@ __global__ void __launch_bounds__(kThreads) gather_rows_bulk_kernel(const Gather
                                                                     int nsegs, int64_t total,
                                                                     const T *__restrict__ src, int64_t ld_src,
                                                                     T *__restrict__ dst, int64_t ld_dst, int K,
-                                                                    int ns, int slot_bytes, int *err)
+                                                                    int ns, int chunk, int slot_bytes, int *err)
 {
     extern __shared__ __align__(128) unsigned char s_dyn[];
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) != 0)
-        return;  // one elected lane per warp issues every copy
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
-    const int64_t it0 = (int64_t)blockIdx.x * kWarpsPerBlock + w;
+    const int64_t wg = (int64_t)blockIdx.x * kWarpsPerBlock + w;
     const uint32_t bytes = (uint32_t)K * (uint32_t)sizeof(T);
     const uint32_t buf0 = smem_addr(s_dyn) + (uint32_t)(w * ns * slot_bytes);
     const uint32_t bar0 = smem_addr(s_dyn) + (uint32_t)(kWarpsPerBlock * ns * slot_bytes) + (uint32_t)(w * ns * 8);
-    for (int q = 0; q < ns; q++)
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar0 + 8u * q) : "memory");
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // barriers visible to the copy engine
-    int sidx_load = 0, sidx_store = 0;
-    auto load = [&](int64_t j) {  // row j of this warp into slot j % ns
-        const T *sp;
-        T *dp;
-        gather_row(segs, single, nsegs, sidx_load, it0 + j * nwarps, src, ld_src, dst, ld_dst, sp, dp);
-        const uint32_t q = (uint32_t)(j % ns);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar0 + 8u * q), "r"(bytes)
-                     : "memory");
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
-                         "r"(buf0 + q * (uint32_t)slot_bytes),
-                     "l"(sp), "r"(bytes), "r"(bar0 + 8u * q)
-                     : "memory");
-    };
-    const int64_t nrows = it0 < total ? (total - 1 - it0) / nwarps + 1 : 0;  // rows of this warp
-    int64_t issued = 0;
-    for (; issued < nrows && issued < ns; issued++)
-        load(issued);
-    uint32_t phase = 0;  // bit q: parity of slot q's next completion
-    bool ok = true;
-    int64_t k = 0;
-    for (; k < nrows; k++) {
-        const uint32_t q = (uint32_t)(k % ns);
-        if (!mbar_wait(bar0 + 8u * q, (phase >> q) & 1u)) {
-            ok = false;
+    if (lane == 0) {
+        for (int q = 0; q < ns; q++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar0 + 8u * q) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // barriers visible to the copy engine
+    }
+    __syncwarp();
+    const int64_t nchunks = (total + chunk - 1) / chunk;
+    uint32_t phase = 0;  // bit q: parity of slot q's next completion (lane 0)
+    int sidx = 0, ok = 1, pending_from = 0, pending_to = 0;
+    for (int64_t c = wg; c < nchunks; c += nwarps) {
+        const int64_t b0 = c * chunk;
+        const int cnt = (int)min((int64_t)chunk, total - b0);
+        const T *sp = nullptr;
+        T *dp = nullptr;
+        if (lane < cnt)
+            gather_row(segs, single, nsegs, sidx, b0 + lane, src, ld_src, dst, ld_dst, sp, dp);
+        for (int j = 0; j < cnt; j++) {  // every row's load at once
+            const T *s_j = reinterpret_cast<const T *>(__shfl_sync(kFull, reinterpret_cast<uintptr_t>(sp), j));
+            if (lane == 0) {
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar0 + 8u * j),
+                             "r"(bytes)
+                             : "memory");
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                        buf0 + (uint32_t)j * (uint32_t)slot_bytes),
+                    "l"(s_j), "r"(bytes), "r"(bar0 + 8u * j)
+                    : "memory");
+            }
+        }
+        for (int j = 0; j < cnt; j++) {  // each row's store as its load lands
+            T *d_j = reinterpret_cast<T *>(__shfl_sync(kFull, reinterpret_cast<uintptr_t>(dp), j));
+            if (lane == 0 && ok) {
+                if (!mbar_wait(bar0 + 8u * j, (phase >> j) & 1u)) {
+                    ok = 0;
+                    pending_from = j;
+                    pending_to = cnt;
+                } else {
+                    phase ^= 1u << j;
+                    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(d_j),
+                                 "r"(buf0 + (uint32_t)j * (uint32_t)slot_bytes), "r"(bytes)
+                                 : "memory");
+                }
+            }
+        }
+        if (lane == 0) {
+            asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+            asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");  // slots free for the next chunk
+        }
+        if (!__shfl_sync(kFull, ok, 0))
             break;
-        }
-        phase ^= 1u << q;
-        const T *sp;
-        T *dp;
-        gather_row(segs, single, nsegs, sidx_store, it0 + k * nwarps, src, ld_src, dst, ld_dst, sp, dp);
-        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dp),
-                     "r"(buf0 + q * (uint32_t)slot_bytes), "r"(bytes)
-                     : "memory");
-        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
-        if (k >= 1 && issued < nrows) {
-            // the store of row k-1 has finished reading its slot: refill it
-            asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
-            load(issued);
-            issued++;
-        }
     }
-    if (!ok) {
-        atomicExch(err, 1);
-        for (int64_t j = k; j < issued; j++) {  // drain the loads still in flight (bounded)
-            const uint32_t q = (uint32_t)(j % ns);
-            if (!mbar_wait(bar0 + 8u * q, (phase >> q) & 1u))
-                break;
-            phase ^= 1u << q;
+    if (lane == 0) {
+        if (!ok) {
+            atomicExch(err, 1);
+            for (int j = pending_from; j < pending_to; j++)  // drain the loads still in flight (bounded)
+                if (!mbar_wait(bar0 + 8u * j, (phase >> j) & 1u))
+                    break;
         }
+        asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
     }
-    asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
 }
 
 // Staged row gather (include/dist_spmm_ppl_batch.cuh:59-73 generalised): one

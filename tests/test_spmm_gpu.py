@@ -447,10 +447,11 @@ def _device_error():
     return code.value
 
 
-@pytest.mark.parametrize("K", [4, 8, 96, 128, 1000, 4096, 3])
+@pytest.mark.parametrize("K", [4, 96, 256, 512, 1000, 4096, 3])
 def test_bulk_gather_copies_rows_exactly(K):
     """The staged gather send[b] = X[idx[b] % npp] through bulk copies (rows of
-    16 B .. 4 KB; 3 columns and 16 KB rows fall back to vectors) gives exactly
+    1 KB .. 4 KB; narrower rows, 3 columns and 16 KB rows take the vector
+    gather) gives exactly
     the rows the vector gather and a plain index copy give, on repeated
     calls, and no bounded wait runs out."""
     npp, P, nemb = 700, 4, 2500
@@ -467,13 +468,13 @@ def test_bulk_gather_copies_rows_exactly(K):
             torch.cuda.synchronize()
             outs.append(out)
     finally:
-        cb.lib().cola_set_gather_bulk(1)
+        cb.lib().cola_set_gather_bulk(0)  # the default
     for o in outs:
         assert torch.equal(o, want)
     assert _device_error() == 0
 
 
-@pytest.mark.parametrize("K,xdt", [(4, torch.float32), (128, torch.float32), (256, torch.bfloat16),
+@pytest.mark.parametrize("K,xdt", [(4, torch.float32), (256, torch.float32), (512, torch.bfloat16),
                                    (1000, torch.float32), (4096, torch.float32), (3, torch.float32)])
 def test_bulk_gather_schedules(case12, K, xdt):
     """BUFFER staging and PIPELINE puts through bulk copies against the vector
@@ -491,7 +492,7 @@ def test_bulk_gather_schedules(case12, K, xdt):
                           gp.spmm(X, schedule=S.SCHEDULE_PIPELINE))
             torch.cuda.synchronize()
     finally:
-        cb.lib().cola_set_gather_bulk(1)
+        cb.lib().cola_set_gather_bulk(0)  # the default
     for j in range(2):
         assert rel(outs[1][j].cpu().numpy(), outs[0][j].cpu().numpy()) <= 1e-6
     assert _device_error() == 0
