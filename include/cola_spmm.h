@@ -345,7 +345,8 @@ typedef struct cola_zip_view {
 cola_status cola_graph_zip_view(const cola_graph *g, int32_t part, cola_zip_view *out);
 
 enum cola_schedule {
-    COLA_SCHEDULE_AUTO = 0,     /* pick by measurement / tuning cache */
+    COLA_SCHEDULE_AUTO = 0,     /* ROWS when the graph has its row view (the fastest measured), else
+                                   PIPELINE for group_size < nparts, else FUSED */
     COLA_SCHEDULE_FUSED = 1,    /* one launch: local CSR + remote CSC, rows staged on chip */
     COLA_SCHEDULE_BUFFER = 2,   /* remote rows gathered into an HBM staging buffer in batches first */
     COLA_SCHEDULE_PIPELINE = 3, /* the reference's multi-stage work-group schedule */
