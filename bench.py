@@ -673,7 +673,7 @@ def run_batched(args):
     t_prep = time.time() - t0
     b.bind(Xs, Ys)
     stream = torch.cuda.current_stream()
-    tuned_ms = b.autotune(reps=3)
+    tuned_ms = b.autotune(reps=3, cache=args.tune_cache)
     cap = torch.cuda.Stream()
     b.capture(stream=cap)
     torch.cuda.synchronize()
@@ -783,6 +783,7 @@ def run_batched(args):
                        "batched_graphs": int(info.batched_graphs), "alg_bytes_per_step": B,
                        "autotuned": {"unroll": int(info.unroll), "grid_pct": int(info.grid_pct),
                                      "blocks_per_sm": int(info.blocks_per_sm),
+                                     "from_cache": bool(b.tuned_from_cache),
                                      "best_ms": tuned_ms},
                        "parallelism": "replicas x{}".format(world),
                        "l2": "inputs larger than L2; no flush", "prep_seconds": round(t_prep, 1)},
@@ -1107,6 +1108,7 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="serving: length of the open-loop phase")
     ap.add_argument("--serve-min-requests", type=int, default=100)
     ap.add_argument("--batch-graphs", type=int, default=512, help="batched workload: number of graphs")
+    ap.add_argument("--tune-cache", default=None, help="batched workload: autotuner cache file (tuned once per shape)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "buffer", "rows"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")

@@ -136,6 +136,7 @@ SIGNATURES = {
     "cola_batch_replay": (I32, [P, P]),
     "cola_batch_set_params": (I32, [P, I32, I32, I32]),
     "cola_batch_autotune": (I32, [P, I32, P, P]),
+    "cola_batch_autotune_cached": (I32, [P, I32, ctypes.c_char_p, P, P, P]),
     "cola_batch_get_info": (I32, [P, P]),
     "cola_server_create": (I32, [P, P]),
     "cola_server_destroy": (I32, [P]),

@@ -2,6 +2,7 @@
 persistent launch (plus one for hub rows), capturable in a CUDA graph, with the
 project's launch-parameter autotuner.  Backed by the cola_batch_* C ABI."""
 import ctypes
+import os
 
 import torch
 
@@ -82,10 +83,20 @@ class Batch:
     def set_params(self, unroll=4, grid_pct=100, blocks_per_sm=4):
         check(lib().cola_batch_set_params(self._h, int(unroll), int(grid_pct), int(blocks_per_sm)))
 
-    def autotune(self, reps=3, stream=None):
-        """Time the launch-parameter candidates on the bound operands; keep the fastest."""
+    def autotune(self, reps=3, stream=None, cache=None):
+        """Time the launch-parameter candidates on the bound operands; keep the
+        fastest.  With `cache` (a file path) a batch tuned before on this device
+        model takes its stored parameters without timing; self.tuned_from_cache
+        tells which happened."""
         ms = ctypes.c_float()
-        check(lib().cola_batch_autotune(self._h, int(reps), _stream(stream), ctypes.byref(ms)))
+        if cache is None:
+            check(lib().cola_batch_autotune(self._h, int(reps), _stream(stream), ctypes.byref(ms)))
+            self.tuned_from_cache = False
+        else:
+            hit = ctypes.c_int32()
+            check(lib().cola_batch_autotune_cached(self._h, int(reps), os.fsencode(cache), _stream(stream),
+                                                   ctypes.byref(ms), ctypes.byref(hit)))
+            self.tuned_from_cache = bool(hit.value)
         return ms.value
 
     @property

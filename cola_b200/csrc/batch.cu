@@ -2,9 +2,11 @@
 // its own dense operands and feature width, in one persistent launch (plus one
 // for hub rows), capturable in a CUDA graph; and the launch-parameter autotuner.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <new>
+#include <string>
 #include <vector>
 
 #include <cuda_bf16.h>
@@ -177,6 +179,48 @@ static cola_status batch_run(cola_batch *b, const cola_spmm_opts *opts, cudaStre
 }  // namespace cola
 
 using namespace cola;
+
+namespace cola {
+// Key of a bound batch in the tuning cache: device model and SM count, then a
+// 64-bit FNV-1a digest of the operand dtypes and, per graph, its rows,
+// entries, width, tasks and hub segments (what the launch's cost depends on).
+static std::string tune_key(const cola_batch *b)
+{
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, b->device) != cudaSuccess)
+        std::strcpy(prop.name, "unknown");
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        for (int i = 0; i < 8; i++) {
+            h ^= (v >> (8 * i)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    };
+    mix((uint64_t)b->xdt);
+    mix((uint64_t)b->ydt);
+    mix(b->graphs.size());
+    for (const cola_graph *g : b->graphs) {
+        mix((uint64_t)g->N);
+        mix((uint64_t)(g->nnz_l + g->nnz_r));
+        mix((uint64_t)g->ntask);
+        mix((uint64_t)g->nseg);
+    }
+    for (const BatchGraph &d : b->h_desc)
+        mix((uint64_t)d.K);
+    for (const cola_batch::Solo &so : b->solo) {
+        mix((uint64_t)so.g);
+        mix((uint64_t)so.K);
+    }
+    std::string name(prop.name);
+    for (char &c : name)
+        if (c == ' ' || c == '\t')
+            c = '_';
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "%s|%d|%016llx", name.c_str(), prop.multiProcessorCount, (unsigned long long)h);
+    return buf;
+}
+
+}  // namespace cola
 
 extern "C" {
 
@@ -417,6 +461,49 @@ done:
     if (s == COLA_SUCCESS && best_ms)
         *best_ms = best;
     return s;
+}
+
+cola_status cola_batch_autotune_cached(cola_batch *b, int32_t reps, const char *cache_path, cola_stream_t stream,
+                                       float *best_ms, int32_t *from_cache)
+{
+    COLA_REQUIRE(b && b->bound, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_batch_autotune_cached: bind the dense operands first");
+    COLA_REQUIRE(cache_path, COLA_ERROR_INVALID_ARGUMENT, "cola_batch_autotune_cached: cache path is NULL");
+    const std::string key = cola::tune_key(b);
+    if (FILE *f = std::fopen(cache_path, "r")) {
+        char line[1024];
+        while (std::fgets(line, sizeof line, f)) {
+            char k[600];
+            int u = 0, gp = 0, bps = 0;
+            float ms = 0.f;
+            if (std::sscanf(line, "%599s %d %d %d %f", k, &u, &gp, &bps, &ms) == 5 && key == k &&
+                (u == 2 || u == 4) && gp >= 10 && gp <= 100 && (bps == 3 || bps == 4)) {
+                std::fclose(f);
+                b->unroll = u;
+                b->grid_pct = gp;
+                b->blocks_per_sm = bps;
+                if (best_ms)
+                    *best_ms = ms;
+                if (from_cache)
+                    *from_cache = 1;
+                return COLA_SUCCESS;
+            }
+        }
+        std::fclose(f);
+    }
+    float ms = 0.f;
+    COLA_TRY(cola_batch_autotune(b, reps, stream, &ms));
+    FILE *f = std::fopen(cache_path, "a");
+    COLA_REQUIRE(f, COLA_ERROR_IO, "cola_batch_autotune_cached: cannot append to %s", cache_path);
+    std::fprintf(f, "%s %d %d %d %.6f\n", key.c_str(), b->unroll, b->grid_pct, b->blocks_per_sm, ms);
+    const bool werr = std::ferror(f) != 0;
+    std::fclose(f);
+    COLA_REQUIRE(!werr, COLA_ERROR_IO, "cola_batch_autotune_cached: cannot write %s", cache_path);
+    if (best_ms)
+        *best_ms = ms;
+    if (from_cache)
+        *from_cache = 0;
+    return COLA_SUCCESS;
 }
 
 }  // extern "C"

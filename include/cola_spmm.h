@@ -420,6 +420,15 @@ cola_status cola_batch_set_params(cola_batch *b, int32_t unroll, int32_t grid_pc
  * each, and keeps the fastest (synchronises `stream`). */
 cola_status cola_batch_autotune(cola_batch *b, int32_t reps, cola_stream_t stream, float *best_ms);
 
+/* cola_batch_autotune with a cache file: when cache_path holds a line for this
+ * batch (same device model and SM count, same graph sizes, widths and dtypes)
+ * its parameters are applied without timing anything (*from_cache = 1);
+ * otherwise the batch is tuned and a line appended (*from_cache = 0).  Text,
+ * one line per batch: "<key> <unroll> <grid_pct> <blocks_per_sm> <best_ms>";
+ * lines that do not parse or hold invalid values are ignored. */
+cola_status cola_batch_autotune_cached(cola_batch *b, int32_t reps, const char *cache_path, cola_stream_t stream,
+                                       float *best_ms, int32_t *from_cache);
+
 typedef struct cola_batch_info {
     int32_t ngraphs, batched_graphs;
     int64_t work_items, hub_items, nnz, device_bytes;

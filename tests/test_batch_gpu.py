@@ -162,3 +162,33 @@ def test_batch_from_existing_graphs_device_built(graphs):
         assert rel(Y.cpu().numpy(), fp64_reference(n, row, col, val, X.cpu().numpy())) <= TOL_F32
     b.close()
     del gs
+
+
+def test_batch_autotune_cache_file(graphs, tmp_path):
+    """The tuning cache: a batch tuned once is tuned from the file the next
+    time (same parameters, no timing); another shape is tuned anew and gets
+    its own line; lines that do not parse are ignored."""
+    cache = tmp_path / "tune.txt"
+    cache.write_text("garbage line\n" + "x 9 9 9 1.0\n")
+
+    def bound(K):
+        b = Batch([g[4] for g in graphs[:4]])
+        b.bind([torch.from_numpy(dense_x(g[0], K, seed=1)).to(DEV) for g in graphs[:4]],
+               [torch.zeros((g[0], K), device=DEV) for g in graphs[:4]])
+        return b
+    b1 = bound(64)
+    b1.autotune(reps=1, cache=str(cache))
+    assert not b1.tuned_from_cache
+    p1 = (b1.info.unroll, b1.info.grid_pct, b1.info.blocks_per_sm)
+    b2 = bound(64)
+    b2.set_params(unroll=2 if p1[0] == 4 else 4, grid_pct=50, blocks_per_sm=3 if p1[2] == 4 else 4)
+    b2.autotune(reps=1, cache=str(cache))
+    assert b2.tuned_from_cache
+    assert (b2.info.unroll, b2.info.grid_pct, b2.info.blocks_per_sm) == p1
+    b3 = bound(128)
+    b3.autotune(reps=1, cache=str(cache))
+    assert not b3.tuned_from_cache
+    lines = [l for l in cache.read_text().splitlines() if l.strip()]
+    assert len(lines) == 4 and all(len(l.split()) == 5 for l in lines[2:])
+    b2.run()
+    torch.cuda.synchronize()
