@@ -6,6 +6,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
@@ -84,12 +85,12 @@ struct FusedArgs {
     bool vec;  // 16-byte vector path allowed
 };
 
-template <typename TR, int LG, int NV, int UNROLL, bool VEC_Y>
+template <typename TR, int LG, int NV, int UNROLL, bool VEC_Y, int MINB = 1>
 static cola_status launch_fused_t(const FusedArgs &a, cudaStream_t st)
 {
     using T = typename dev::ElemOf<TR>::T;
     constexpr int W = LG * NV * TR::E;
-    auto fn = dev::fused_spmm_kernel<TR, LG, NV, UNROLL, VEC_Y>;
+    auto fn = dev::fused_spmm_kernel<TR, LG, NV, UNROLL, VEC_Y, MINB>;
     // one warp per chunk (as many blocks as the chunks need): measured 11 %
     // faster than a persistent grid for this kernel, whose items are short
     const int64_t gx = std::max<int64_t>(1, (a.total + dev::kWarpsPerBlock - 1) / dev::kWarpsPerBlock);
@@ -116,8 +117,15 @@ static cola_status launch_fused_geo(const FusedArgs &a, int V, cudaStream_t st)
         return launch_fused_t<TR, 8, 1, 4, VEC_Y>(a, st);
     if (V <= 16)
         return launch_fused_t<TR, 16, 1, 4, VEC_Y>(a, st);
-    if (V <= 32)
+    if (V <= 32) {
+        // FP32 rows of 65-128 features (K = 128 in the reference's runs): one row in
+        // flight per warp and 32 registers, so 8 blocks (64 warps) fit an SM --
+        // measured 4 % faster than 2 rows in flight at 6 blocks on the
+        // per-partition launches of an R-MAT scale-20 graph at K = 128
+        if constexpr (std::is_same<TR, dev::VecTraits<float>>::value)
+            return launch_fused_t<TR, 32, 1, 1, VEC_Y, 8>(a, st);
         return launch_fused_t<TR, 32, 1, 2, VEC_Y>(a, st);  // 2 rows in flight: fewer registers, more warps
+    }
     if (V <= 64)
         return launch_fused_t<TR, 32, 2, 2, VEC_Y>(a, st);
     return launch_fused_t<TR, 32, 4, 2, VEC_Y>(a, st);

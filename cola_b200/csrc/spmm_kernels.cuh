@@ -137,9 +137,10 @@ __device__ __forceinline__ const PartDesc *find_part(const PartDesc *parts, int 
 
 // The fused partitioned SpMM: items [0, total) over all parts; item i of part
 // d is local chunk d.l_begin + i when i < d.l_num, else remote chunk
-// d.r_begin + (i - d.l_num).  blockIdx.y selects the feature tile.
-template <typename TR, int LG, int NV, int UNROLL, bool VEC_Y>
-__global__ void __launch_bounds__(kThreads) fused_spmm_kernel(const PartDesc *__restrict__ parts,
+// d.r_begin + (i - d.l_num).  blockIdx.y selects the feature tile.  MINB is
+// the number of blocks per SM the registers must allow.
+template <typename TR, int LG, int NV, int UNROLL, bool VEC_Y, int MINB = 1>
+__global__ void __launch_bounds__(kThreads, MINB) fused_spmm_kernel(const PartDesc *__restrict__ parts,
                                                               const __grid_constant__ PartDesc single, int nparts,
                                                               int64_t total,
                                                               const typename ElemOf<TR>::T *__restrict__ X,
