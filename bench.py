@@ -102,8 +102,19 @@ class Clocks:
         self.index = index
         self.proc = None
         self.path = None
+        self.lo = self.hi = 0
+        self.t0 = self.t1 = 0.0
+
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return sum(1 for line in f if line.endswith("\n"))
+        except (OSError, TypeError):
+            return 0
 
     def start(self):
+        """Starts nvidia-smi sampling every 200 ms and returns once its first
+        sample is written, so that the samples after it cover the load."""
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -112,11 +123,33 @@ class Clocks:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        t = time.time()
+        while time.time() - t < 5.0 and self._lines() == 0 and self.proc.poll() is None:
+            time.sleep(0.02)
+        self.lo = self._lines()
+        self.t0 = time.time()
+
+    def hold(self, step=None, min_s=1.2):
+        """Ends the sampled load window.  A timed region shorter than two
+        sampling periods would leave nvidia-smi nothing to see, so the same
+        work (`step`, untimed) keeps running until the window is min_s long;
+        the samples between start() and here are the ones reported."""
+        if self.proc is None:
+            return
+        if step is not None:
+            import torch
+            while time.time() - self.t0 < min_s:
+                step()
+                torch.cuda.synchronize()
+        self.t1 = time.time()
+        self.hi = self._lines()
 
     def stop(self):
         if self.proc is None:
             return None
-        time.sleep(0.25)
+        if self.hi == 0:
+            self.hold()
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -129,6 +162,8 @@ class Clocks:
                 if len(p) >= 9:
                     rows.append(p)
         os.unlink(self.path)
+        if self.hi > self.lo:
+            rows = rows[self.lo:self.hi]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -136,7 +171,8 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "window_s": round(self.t1 - self.t0, 3),
+                "window": "the timed region, then the same work untimed until the window is 1.2 s"}
 
 
 # ---------------------------------------------------------------------------
@@ -375,6 +411,7 @@ def run_ours(args, w):
     k_list = [a.elapsed_time(b) for a, b in kev]
     k_ms = max_over_ranks(sum(k_list) / len(k_list))
     k_med = max_over_ranks(statistics.median(k_list))
+    clocks.hold(step)
     clk = clocks.stop()
     del Yacc
 
@@ -698,6 +735,7 @@ def run_batched(args):
         b.replay(stream)
     e1.record(stream)
     torch.cuda.synchronize()
+    clocks.hold(lambda: b.replay(stream))
     clk = clocks.stop()
     ms = world_reduce(e0.elapsed_time(e1) / args.steps, dev, "max")
     # e2e: per graph pinned X -> device, the captured launch, Y -> pinned host;
@@ -1022,6 +1060,7 @@ def run_prep(args):
         build(rd, cd, vd).close()
     ev[1].record(stream)
     torch.cuda.synchronize()
+    clocks.hold(lambda: build(rd, cd, vd).close())
     clk = clocks.stop()
     ms = world_reduce(ev[0].elapsed_time(ev[1]) / args.steps, dev, "max")
     # end to end: pinned host COO -> device, build, partitions in host memory
