@@ -402,7 +402,9 @@ def run_ours(args, w):
     # the SpMM kernels alone: for the fused schedule in accumulate mode (the same
     # launch without the Y zeroing); the row-major schedule has no zeroing
     Yacc = torch.zeros((n, K), dtype=torch.float32, device=dev) if eff == S.SCHEDULE_FUSED else Y
-    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    # at least 50 launches, so that the median is taken over 50 or more runs
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(max(args.steps, 50))]
     for a, b in kev:
         a.record(stream)
         g.spmm(X, Yacc, accumulate=(eff == S.SCHEDULE_FUSED), schedule=sched, unroll=args.unroll, min_blocks=args.min_blocks, stream=stream)
@@ -509,7 +511,7 @@ def run_ours(args, w):
                    "prep_seconds": round(t_prep, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
-                     "kernel_ms": k_ms, "kernel_ms_median": k_med, "frac_of_8TBs": achieved / 8000.0,
+                     "kernel_ms": k_ms, "kernel_ms_median": k_med, "kernel_runs": len(k_list), "frac_of_8TBs": achieved / 8000.0,
                      # what must cross DRAM at least: indices and values once, X and Y once
                      "compulsory_bytes": int(info.nnz) * 8 + n * K * (s_x + s_y),
                      "traffic_over_compulsory": None if traffic is None else
