@@ -66,6 +66,8 @@ struct Group {
     int slot = 0;
     int64_t bytes = 0;
     bool completed = false;
+    bool timed = false;
+    float ms[3] = {0, 0, 0};  // copy-in, launch, copy-out (read when retired)
 };
 
 }  // namespace
@@ -208,20 +210,29 @@ static void scheduler(cola_server *S)
                     return true;
             return false;
         });
-        // retire
-        for (Group *G : S->finished) {
-            Slot &sl = S->slots[(size_t)G->slot];
-            if (G->reqs.front()->t_submit >= S->t_window) {
-                float ms[3] = {0, 0, 0};
-                bool ok = true;
+        // retire.  The phase timings are read without the lock: no CUDA call
+        // is ever made under S->mu, which the completion callbacks (run by
+        // the driver) take.  A finished group's slot stays busy until it is
+        // retired below, so its events are not recorded again meanwhile.
+        std::vector<Group *> done;
+        done.swap(S->finished);
+        if (!done.empty()) {
+            lk.unlock();
+            for (Group *G : done) {
+                Slot &sl = S->slots[(size_t)G->slot];
+                G->timed = true;
                 for (int k = 0; k < 3; k++)
-                    ok = ok && cudaEventElapsedTime(&ms[k], sl.ev[k], sl.ev[k + 1]) == cudaSuccess;
-                if (ok) {
-                    S->copy_in_ms_sum += ms[0];
-                    S->kernel_ms_sum += ms[1];
-                    S->copy_out_ms_sum += ms[2];
-                    S->timed_groups++;
-                }
+                    G->timed = G->timed && cudaEventElapsedTime(&G->ms[k], sl.ev[k], sl.ev[k + 1]) == cudaSuccess;
+            }
+            lk.lock();
+        }
+        for (Group *G : done) {
+            Slot &sl = S->slots[(size_t)G->slot];
+            if (G->reqs.front()->t_submit >= S->t_window && G->timed) {
+                S->copy_in_ms_sum += G->ms[0];
+                S->kernel_ms_sum += G->ms[1];
+                S->copy_out_ms_sum += G->ms[2];
+                S->timed_groups++;
             }
             sl.busy = nullptr;
             S->used -= G->bytes;
@@ -237,9 +248,8 @@ static void scheduler(cola_server *S)
             }
             delete G;
         }
-        if (!S->finished.empty())
+        if (!done.empty())
             S->cv_done.notify_all();
-        S->finished.clear();
         if (S->stop && S->pending.empty() && S->inflight == 0)
             break;
         // admit
@@ -287,10 +297,9 @@ static void scheduler(cola_server *S)
             // must not block the completion callbacks, which take the lock
             lk.unlock();
             const cola_status st = launch_group(S, G);
-            lk.lock();
             if (st != COLA_SUCCESS) {
                 // the group never reaches its callback: release what it queued
-                // and fail it here
+                // (still without the lock) and fail it below
                 cudaStream_t sst = S->slots[(size_t)slot].stream;
                 for (Request *r : G->reqs) {
                     if (r->dX)
@@ -302,6 +311,9 @@ static void scheduler(cola_server *S)
                     r->dX = r->dY = nullptr;
                     r->dws = nullptr;
                 }
+            }
+            lk.lock();
+            if (st != COLA_SUCCESS) {
                 S->slots[(size_t)slot].busy = nullptr;
                 S->used -= G->bytes;
                 S->inflight -= (int32_t)G->reqs.size();
@@ -426,11 +438,14 @@ cola_status cola_server_register(cola_server *S, const cola_partition_set *parts
                  "cola_server_register: server lives on device %d, current device is %d", S->device, cur);
     cola_graph *g = nullptr;
     COLA_TRY(graph_upload(parts, opts, g, nullptr));
-    std::lock_guard<std::mutex> lk(S->mu);
+    std::unique_lock<std::mutex> lk(S->mu);
     if (S->used + (int64_t)g->dbytes > S->budget) {
+        const long long used = (long long)S->used, budget = (long long)S->budget;
+        lk.unlock();  // no CUDA call under the lock
+        const size_t need = g->dbytes;
         graph_release(g);
         return fail(COLA_ERROR_BUDGET, "cola_server_register: graph needs %zu bytes, %lld of %lld bytes in use",
-                    g->dbytes, (long long)S->used, (long long)S->budget);
+                    need, used, budget);
     }
     S->used += (int64_t)g->dbytes;
     S->graph_bytes += (int64_t)g->dbytes;
@@ -453,12 +468,14 @@ cola_status cola_server_register_graph(cola_server *S, cola_graph *g, int32_t *g
                     "cola_server_register_graph: the graph needs its row view and the server's device %d (it "
                     "lives on %d)", S->device, dev);
     }
-    std::lock_guard<std::mutex> lk(S->mu);
+    std::unique_lock<std::mutex> lk(S->mu);
     if (S->used + (int64_t)g->dbytes > S->budget) {
+        const long long used = (long long)S->used, budget = (long long)S->budget;
+        lk.unlock();  // no CUDA call under the lock
         const size_t need = g->dbytes;
         graph_release(g);
         return fail(COLA_ERROR_BUDGET, "cola_server_register_graph: graph needs %zu bytes, %lld of %lld bytes in use",
-                    need, (long long)S->used, (long long)S->budget);
+                    need, used, budget);
     }
     S->used += (int64_t)g->dbytes;
     S->graph_bytes += (int64_t)g->dbytes;
