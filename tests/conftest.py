@@ -15,6 +15,21 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
 
 
+# A GPU test gets 300 s (the whole GPU suite takes about 20 s on a B200): one
+# that stalls ends the run with every thread's stack printed, instead of holding
+# the GPU until an outer limit (pytest-timeout's thread method also ends a run
+# whose main thread is blocked inside a C call).
+GPU_TEST_SECONDS = 300
+
+
+def pytest_collection_modifyitems(config, items):
+    if not config.pluginmanager.hasplugin("timeout"):
+        return
+    for item in items:
+        if item.get_closest_marker("gpu") is not None and item.get_closest_marker("timeout") is None:
+            item.add_marker(pytest.mark.timeout(GPU_TEST_SECONDS, method="thread"))
+
+
 def _ensure_oracle():
     so = os.path.join(REPO, "oracle", "liboracle.so")
     if not os.path.exists(so):
