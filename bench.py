@@ -33,6 +33,8 @@ import time
 import numpy as np
 
 REPO = os.path.dirname(os.path.abspath(__file__))
+# a serving request not back within this long is an error, not an endless wait
+WAIT_MS = 600_000
 sys.path.insert(0, REPO)
 
 WORKLOADS = {
@@ -914,15 +916,15 @@ def run_serving(args):
     # server's memory pool to its working size), then the saturation rate: a
     # burst submitted at once
     for _ in range(max(args.warmup, 3)):
-        submit(*draw()).wait()
+        submit(*draw()).wait(timeout_ms=WAIT_MS)
     for r in [submit(*draw()) for _ in range(args.serve_burst)]:
-        r.wait()
+        r.wait(timeout_ms=WAIT_MS)
     world_barrier()
     burst = [draw() for _ in range(args.serve_burst)]
     tb = time.perf_counter()
     reqs = [submit(*d) for d in burst]
     for r in reqs:
-        r.wait()
+        r.wait(timeout_ms=WAIT_MS)
     cap = len(burst) / (time.perf_counter() - tb)
     # open loop: Poisson arrivals at a fraction of the saturation rate
     rate = args.serve_load * cap
@@ -942,7 +944,7 @@ def run_serving(args):
             time.sleep(delay)
         reqs.append(submit(*d))
     for r in reqs:
-        r.wait()
+        r.wait(timeout_ms=WAIT_MS)
     wall = time.perf_counter() - ts
     clk = clocks.stop()
     st = srv.stats()
