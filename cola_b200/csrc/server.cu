@@ -21,6 +21,7 @@
 #include "batch.h"
 #include "common.h"
 #include "graph.h"
+#include "server_policy.h"
 
 using cola::dev::BatchGraph;
 
@@ -189,11 +190,11 @@ static void CUDART_CB group_done_cb(void *p)
 }
 
 // Scheduler: retire finished groups (return their memory to the budget, wake
-// waiters), then admit pending requests into free slots.  Admission is FIFO:
-// the oldest pending request opens a group of its (K, dtypes) key, later
-// pending requests with the same key join while the group (request count and
-// copy bytes) and the budget have room; a head request that does not fit waits
-// for memory to free up.  The copy-byte cap keeps large requests in groups of
+// waiters), then admit pending requests into free slots, a group at a time as
+// pick_group (server_policy.h) chooses: FIFO, the head opening a group of its
+// (K, dtypes) key that later requests of the key join while the request count,
+// the copy bytes and the budget allow; a head that does not fit waits for
+// memory to free up.  The copy-byte cap keeps large requests in groups of
 // their own, so one slot's copy-in overlaps another's launch and copy-out.
 static void scheduler(cola_server *S)
 {
@@ -201,14 +202,12 @@ static void scheduler(cola_server *S)
     std::unique_lock<std::mutex> lk(S->mu);
     while (true) {
         S->cv_sched.wait(lk, [&] {
-            if (!S->finished.empty() || (S->stop && S->inflight == 0))
-                return true;
-            if (S->pending.empty())
-                return false;
+            bool free_slot = false;
             for (const Slot &sl : S->slots)
-                if (!sl.busy)
-                    return true;
-            return false;
+                free_slot = free_slot || !sl.busy;
+            return scheduler_has_work(!S->finished.empty(), S->stop, S->inflight, !S->pending.empty(),
+                                      S->pending.empty() ? 0 : S->pending.front()->bytes, S->used, S->budget,
+                                      free_slot);
         });
         // retire.  The phase timings are read without the lock: no CUDA call
         // is ever made under S->mu, which the completion callbacks (run by
@@ -262,27 +261,19 @@ static void scheduler(cola_server *S)
                 }
             if (slot < 0)
                 break;
-            Request *head = S->pending.front();
-            if (S->used + head->bytes > S->budget)
-                break;  // wait for memory
+            const std::vector<size_t> pick = pick_group(S->pending, S->used, S->budget, S->max_group, S->group_bytes);
+            if (pick.empty())
+                break;  // the head waits for memory
             Group *G = new Group();
             G->slot = slot;
-            int64_t copy = 0;
-            for (auto it = S->pending.begin(); it != S->pending.end() && (int32_t)G->reqs.size() < S->max_group &&
-                                               copy < S->group_bytes;) {
-                Request *r = *it;
-                if (r->K == head->K && r->xdt == head->xdt && r->ydt == head->ydt &&
-                    S->used + G->bytes + r->bytes <= S->budget &&
-                    (G->reqs.empty() || copy + r->copy_bytes <= S->group_bytes)) {
-                    G->reqs.push_back(r);
-                    G->bytes += r->bytes;
-                    copy += r->copy_bytes;
-                    r->state = kRunning;
-                    it = S->pending.erase(it);
-                } else {
-                    ++it;
-                }
+            for (size_t i : pick) {
+                Request *r = S->pending[i];
+                G->reqs.push_back(r);
+                G->bytes += r->bytes;
+                r->state = kRunning;
             }
+            for (size_t k = pick.size(); k-- > 0;)  // back to front: earlier positions stay valid
+                S->pending.erase(S->pending.begin() + (std::ptrdiff_t)pick[k]);
             S->used += G->bytes;
             S->peak_used = std::max(S->peak_used, S->used);
             S->inflight += (int32_t)G->reqs.size();
@@ -570,6 +561,7 @@ cola_status cola_server_cancel(cola_server *S, uint64_t request_id)
     r->status = COLA_ERROR_CANCELLED;
     S->cancelled++;
     S->cv_done.notify_all();
+    S->cv_sched.notify_all();  // a new head may fit where the cancelled one did not
     return COLA_SUCCESS;
 }
 

@@ -1,0 +1,128 @@
+"""The serving loop's admission policy (cola_b200/csrc/server_policy.h, the
+functions the scheduler thread calls), compiled on the CPU.  pick_group is
+checked on seeded random queues against the properties it promises: FIFO head
+first, one (K, dtypes) key per group, the request-count, copy-byte and
+memory-budget caps, and no request left out that would have fitted when it was
+considered.  scheduler_has_work is checked over its whole truth table; in
+particular a head that does not fit in the budget must not count as work (the
+scheduler would spin holding the lock the completion callback needs)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def policy_exe(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("policy") / "server_policy_main")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-Werror",
+                           "-I", os.path.join(REPO, "cola_b200", "csrc"),
+                           os.path.join(REPO, "tests", "server_policy_main.cpp"), "-o", exe])
+    return exe
+
+
+def scenarios(seed, count):
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for _ in range(count):
+        n = int(rng.integers(0, 40))
+        keys = [(int(k), int(x), int(y)) for k, x, y in
+                zip(rng.choice([16, 64, 256], n), rng.integers(0, 2, n), rng.integers(0, 2, n))]
+        if n and rng.random() < 0.5:  # often one key dominates
+            keys = [keys[0] if rng.random() < 0.8 else k for k in keys]
+        bytes_ = rng.integers(1, 1000, n).astype(np.int64)
+        copy = rng.integers(1, 800, n).astype(np.int64)
+        used = int(rng.integers(0, 2000))
+        budget = used + int(rng.integers(0, 6000))
+        max_group = int(rng.integers(1, 17))
+        group_bytes = int(rng.integers(1, 4000))
+        reqs = [(k[0], k[1], k[2], int(b), int(c)) for k, b, c in zip(keys, bytes_, copy)]
+        out.append((used, budget, max_group, group_bytes, reqs))
+    return out
+
+
+def run(exe, cases):
+    lines = [str(len(cases))]
+    for used, budget, max_group, group_bytes, reqs in cases:
+        lines.append("{} {} {} {} {}".format(used, budget, max_group, group_bytes, len(reqs)))
+        lines += ["{} {} {} {} {}".format(*r) for r in reqs]
+    res = subprocess.run([exe], input="\n".join(lines) + "\n", capture_output=True, text=True, check=True)
+    picks = []
+    for line in res.stdout.splitlines():
+        picks.append([] if line.strip() == "-" else [int(v) for v in line.split()])
+    assert len(picks) == len(cases)
+    return picks
+
+
+def check(case, pick):
+    used, budget, max_group, group_bytes, reqs = case
+    if not reqs or used + reqs[0][3] > budget:
+        assert pick == []  # nothing pending, or the head waits for memory
+        return
+    assert pick and pick[0] == 0  # FIFO: the head opens the group
+    assert pick == sorted(set(pick))
+    key = reqs[0][:3]
+    assert all(reqs[i][:3] == key for i in pick)
+    assert len(pick) <= max_group
+    assert used + sum(reqs[i][3] for i in pick) <= budget
+    assert len(pick) == 1 or sum(reqs[i][4] for i in pick) <= group_bytes
+    # nothing left out that fitted when the scan reached it
+    chosen = set(pick)
+    n_in, b_in, c_in = 0, 0, 0
+    for i, r in enumerate(reqs):
+        if n_in >= max_group or c_in >= group_bytes:
+            break  # the scan stops here
+        fits = (r[:3] == key and used + b_in + r[3] <= budget and (n_in == 0 or c_in + r[4] <= group_bytes))
+        assert fits == (i in chosen), (i, r, pick)
+        if fits:
+            n_in, b_in, c_in = n_in + 1, b_in + r[3], c_in + r[4]
+    assert n_in == len(pick)
+
+
+def test_policy_properties_on_random_queues(policy_exe):
+    cases = scenarios(seed=11, count=3000)
+    for case, pick in zip(cases, run(policy_exe, cases)):
+        check(case, pick)
+
+
+def test_policy_edge_cases(policy_exe):
+    big = (64, 0, 0, 10 ** 12, 10 ** 12)
+    small = (64, 0, 0, 10, 10)
+    cases = [
+        (0, 100, 4, 100, []),                                   # nothing pending
+        (0, 100, 4, 100, [(64, 0, 0, 101, 1)]),                 # the head cannot fit yet
+        (0, 10 ** 13, 4, 100, [big, small, small]),             # a huge head still gets a group of its own
+        (0, 100, 1, 10 ** 6, [small, small, small]),            # max_group 1
+        (0, 35, 8, 10 ** 6, [small, small, small, small]),      # the budget admits three
+        (0, 10 ** 6, 8, 25, [small, small, small, small]),      # the copy cap admits two
+        (0, 10 ** 6, 8, 10 ** 6, [small, (16, 0, 0, 1, 1), small, (64, 1, 0, 1, 1), small]),  # keys
+    ]
+    picks = run(policy_exe, cases)
+    assert picks == [[], [], [0], [0], [0, 1, 2], [0, 1], [0, 2, 4]]
+    for case, pick in zip(cases, picks):
+        check(case, pick)
+
+
+def test_scheduler_wake_condition(policy_exe):
+    import itertools
+    rows, want = [], []
+    for finished, stop, inflight, pending, fits, free_slot in itertools.product([0, 1], [0, 1], [0, 2], [0, 1],
+                                                                              [0, 1], [0, 1]):
+        used, budget = 500, 1000
+        head = 400 if fits else 600
+        rows.append("{} {} {} {} {} {} {} {}".format(finished, stop, inflight, pending, head if pending else 0, used,
+                                                     budget, free_slot))
+        want.append(int(bool(finished) or (bool(stop) and inflight == 0) or
+                        (bool(pending) and bool(fits) and bool(free_slot))))
+    res = subprocess.run([policy_exe, "wake"], input="{}\n{}\n".format(len(rows), "\n".join(rows)),
+                         capture_output=True, text=True, check=True)
+    got = [int(v) for v in res.stdout.split()]
+    assert got == want
+    # the stall this rules out: requests queued behind a head that waits for
+    # memory, a slot free, nothing finished yet -> the scheduler must sleep
+    res = subprocess.run([policy_exe, "wake"], input="1\n0 0 1 1 600 500 1000 1\n", capture_output=True, text=True,
+                         check=True)
+    assert res.stdout.split() == ["0"]
