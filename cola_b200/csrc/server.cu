@@ -32,7 +32,11 @@ double now_s()
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-enum ReqState { kPending = 0, kRunning = 1, kDone = 2, kCancelled = 3, kFailed = 4 };
+using cola::kCancelled;
+using cola::kDone;
+using cola::kFailed;
+using cola::kPending;
+using cola::kRunning;
 
 struct Request {
     uint64_t id = 0;
@@ -51,7 +55,8 @@ struct Request {
     float *dws = nullptr;
 };
 
-struct Group;
+struct Request;
+using Group = cola::SchedGroup<Request>;
 
 struct Slot {
     cudaStream_t stream = nullptr;
@@ -60,15 +65,6 @@ struct Slot {
     BatchGraph *h_desc = nullptr;  // staging (pinned)
     int cap = 0;
     cudaEvent_t ev[4] = {};  // group start, X copied in, launch done, Y copied out
-};
-
-struct Group {
-    std::vector<Request *> reqs;
-    int slot = 0;
-    int64_t bytes = 0;
-    bool completed = false;
-    bool timed = false;
-    float ms[3] = {0, 0, 0};  // copy-in, launch, copy-out (read when retired)
 };
 
 }  // namespace
@@ -177,17 +173,38 @@ static cola_status launch_group(cola_server *S, Group *G)
 static void CUDART_CB group_done_cb(void *p)
 {
     HostCbArg *a = static_cast<HostCbArg *>(p);
-    const double t = now_s();
-    {
-        std::lock_guard<std::mutex> lk(a->s->mu);
-        for (Request *r : a->g->reqs)
-            r->t_done = t;
-        a->g->completed = true;
-        a->s->finished.push_back(a->g);
-    }
-    a->s->cv_sched.notify_all();
+    group_finished(a->s, a->g, now_s());
     delete a;
 }
+
+// The device hooks of the scheduler loop (run_scheduler in server_policy.h).
+struct CudaSched {
+    static cola_status launch(cola_server *S, Group *G) { return launch_group(S, G); }
+    // phase timings from the slot's events (the slot stays busy until the
+    // group is retired, so they are not recorded again meanwhile)
+    static void read_timings(cola_server *S, Group *G)
+    {
+        Slot &sl = S->slots[(size_t)G->slot];
+        G->timed = true;
+        for (int k = 0; k < 3; k++)
+            G->timed = G->timed && cudaEventElapsedTime(&G->ms[k], sl.ev[k], sl.ev[k + 1]) == cudaSuccess;
+    }
+    static void release_failed(cola_server *S, Group *G)
+    {
+        cudaStream_t st = S->slots[(size_t)G->slot].stream;
+        for (Request *r : G->reqs) {
+            if (r->dX)
+                cudaFreeAsync(r->dX, st);
+            if (r->dY)
+                cudaFreeAsync(r->dY, st);
+            if (r->dws)
+                cudaFreeAsync(r->dws, st);
+            r->dX = r->dY = nullptr;
+            r->dws = nullptr;
+        }
+    }
+    static double now() { return now_s(); }
+};
 
 // Scheduler: retire finished groups (return their memory to the budget, wake
 // waiters), then admit pending requests into free slots, a group at a time as
@@ -199,125 +216,7 @@ static void CUDART_CB group_done_cb(void *p)
 static void scheduler(cola_server *S)
 {
     cudaSetDevice(S->device);
-    std::unique_lock<std::mutex> lk(S->mu);
-    while (true) {
-        S->cv_sched.wait(lk, [&] {
-            bool free_slot = false;
-            for (const Slot &sl : S->slots)
-                free_slot = free_slot || !sl.busy;
-            return scheduler_has_work(!S->finished.empty(), S->stop, S->inflight, !S->pending.empty(),
-                                      S->pending.empty() ? 0 : S->pending.front()->bytes, S->used, S->budget,
-                                      free_slot);
-        });
-        // retire.  The phase timings are read without the lock: no CUDA call
-        // is ever made under S->mu, which the completion callbacks (run by
-        // the driver) take.  A finished group's slot stays busy until it is
-        // retired below, so its events are not recorded again meanwhile.
-        std::vector<Group *> done;
-        done.swap(S->finished);
-        if (!done.empty()) {
-            lk.unlock();
-            for (Group *G : done) {
-                Slot &sl = S->slots[(size_t)G->slot];
-                G->timed = true;
-                for (int k = 0; k < 3; k++)
-                    G->timed = G->timed && cudaEventElapsedTime(&G->ms[k], sl.ev[k], sl.ev[k + 1]) == cudaSuccess;
-            }
-            lk.lock();
-        }
-        for (Group *G : done) {
-            Slot &sl = S->slots[(size_t)G->slot];
-            if (G->reqs.front()->t_submit >= S->t_window && G->timed) {
-                S->copy_in_ms_sum += G->ms[0];
-                S->kernel_ms_sum += G->ms[1];
-                S->copy_out_ms_sum += G->ms[2];
-                S->timed_groups++;
-            }
-            sl.busy = nullptr;
-            S->used -= G->bytes;
-            S->inflight -= (int32_t)G->reqs.size();
-            for (Request *r : G->reqs) {
-                r->state = kDone;
-                if (r->t_submit >= S->t_window) {
-                    S->completed++;
-                    S->lat_ms.push_back((r->t_done - r->t_submit) * 1e3);
-                    S->queue_ms_sum += (r->t_launch - r->t_submit) * 1e3;
-                    S->t_last = std::max(S->t_last, r->t_done);
-                }
-            }
-            delete G;
-        }
-        if (!done.empty())
-            S->cv_done.notify_all();
-        if (S->stop && S->pending.empty() && S->inflight == 0)
-            break;
-        // admit
-        while (!S->pending.empty()) {
-            int slot = -1;
-            for (size_t i = 0; i < S->slots.size(); i++)
-                if (!S->slots[i].busy) {
-                    slot = (int)i;
-                    break;
-                }
-            if (slot < 0)
-                break;
-            const std::vector<size_t> pick = pick_group(S->pending, S->used, S->budget, S->max_group, S->group_bytes);
-            if (pick.empty())
-                break;  // the head waits for memory
-            Group *G = new Group();
-            G->slot = slot;
-            for (size_t i : pick) {
-                Request *r = S->pending[i];
-                G->reqs.push_back(r);
-                G->bytes += r->bytes;
-                r->state = kRunning;
-            }
-            for (size_t k = pick.size(); k-- > 0;)  // back to front: earlier positions stay valid
-                S->pending.erase(S->pending.begin() + (std::ptrdiff_t)pick[k]);
-            S->used += G->bytes;
-            S->peak_used = std::max(S->peak_used, S->used);
-            S->inflight += (int32_t)G->reqs.size();
-            S->max_inflight = std::max(S->max_inflight, S->inflight);
-            S->max_group_seen = std::max(S->max_group_seen, (int32_t)G->reqs.size());
-            S->groups_launched++;
-            S->slots[(size_t)slot].busy = G;
-            const double t_launch = now_s();
-            for (Request *r : G->reqs)
-                r->t_launch = t_launch;
-            // launch without the lock: a CUDA call that waits on the device
-            // must not block the completion callbacks, which take the lock
-            lk.unlock();
-            const cola_status st = launch_group(S, G);
-            if (st != COLA_SUCCESS) {
-                // the group never reaches its callback: release what it queued
-                // (still without the lock) and fail it below
-                cudaStream_t sst = S->slots[(size_t)slot].stream;
-                for (Request *r : G->reqs) {
-                    if (r->dX)
-                        cudaFreeAsync(r->dX, sst);
-                    if (r->dY)
-                        cudaFreeAsync(r->dY, sst);
-                    if (r->dws)
-                        cudaFreeAsync(r->dws, sst);
-                    r->dX = r->dY = nullptr;
-                    r->dws = nullptr;
-                }
-            }
-            lk.lock();
-            if (st != COLA_SUCCESS) {
-                S->slots[(size_t)slot].busy = nullptr;
-                S->used -= G->bytes;
-                S->inflight -= (int32_t)G->reqs.size();
-                for (Request *r : G->reqs) {
-                    r->state = kFailed;
-                    r->status = st;
-                    S->failed++;
-                }
-                delete G;
-                S->cv_done.notify_all();
-            }
-        }
-    }
+    run_scheduler<cola_server, CudaSched>(S);
 }
 
 }  // namespace cola

@@ -1,5 +1,6 @@
-// Admission policy of the serving loop, free of CUDA so that it can be tested
-// on its own: which pending requests form the next group.
+// The serving loop's scheduling, free of CUDA so that it can be tested on its
+// own: the admission policy (which pending requests form the next group), the
+// wake condition, and the scheduler loop itself over device hooks.
 //
 // FIFO: the oldest pending request (the head) opens a group when the budget
 // has room for it next to what is already in flight.  Later pending requests
@@ -11,11 +12,30 @@
 //   * the budget has room for the group with the request.
 // A request that does not fit is skipped, not dropped: it stays pending.
 #pragma once
+#include <algorithm>
+#include <condition_variable>
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
+#include <type_traits>
 #include <vector>
 
 namespace cola {
+
+// Life of a request: pending (queued) -> running (admitted in a group) ->
+// done | failed, or pending -> cancelled.
+enum ReqState { kPending = 0, kRunning = 1, kDone = 2, kCancelled = 3, kFailed = 4 };
+
+// A group: requests admitted together into one slot.
+template <typename Req>
+struct SchedGroup {
+    std::vector<Req *> reqs;
+    int slot = 0;
+    int64_t bytes = 0;
+    bool completed = false;
+    bool timed = false;
+    float ms[3] = {0, 0, 0};  // copy-in, launch, copy-out (read when retired)
+};
 
 // R: any type with fields K, xdt, ydt (compared for equality), bytes (device
 // bytes while in flight) and copy_bytes (host <-> device bytes).  Returns the
@@ -58,6 +78,140 @@ inline bool scheduler_has_work(bool finished, bool stop, int32_t inflight, bool 
     if (!pending || used + head_bytes > budget)
         return false;
     return free_slot;
+}
+
+// Reports a group's device work as complete: called once per launched group,
+// from any thread (the CUDA driver's callback thread in the server), never
+// with S->mu held.
+template <typename Srv, typename Group>
+void group_finished(Srv *S, Group *G, double t)
+{
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (auto *r : G->reqs)
+            r->t_done = t;
+        G->completed = true;
+        S->finished.push_back(G);
+    }
+    S->cv_sched.notify_all();
+}
+
+// The scheduler thread: retire finished groups (return their memory to the
+// budget, wake waiters), then admit pending requests into free slots, a group
+// at a time as pick_group chooses; sleep while scheduler_has_work says there
+// is nothing to do; end once stopped with nothing in flight.  Srv holds the
+// server's state (mu, cv_sched, cv_done, pending, finished, slots[].busy,
+// used, budget, inflight, stop, the group caps and the statistics).  B holds
+// the device hooks, none of them called with S->mu held:
+//   B::launch(S, G)          queue the group's work (0 = queued); the work's
+//                            completion must call group_finished(S, G, t)
+//   B::read_timings(S, G)    fill G->timed and G->ms for a finished group
+//   B::release_failed(S, G)  free what a launch that failed had queued
+//   B::now()                 seconds
+template <typename Srv, typename B>
+void run_scheduler(Srv *S)
+{
+    using Group = typename std::remove_pointer<typename decltype(S->finished)::value_type>::type;
+    std::unique_lock<std::mutex> lk(S->mu);
+    while (true) {
+        S->cv_sched.wait(lk, [&] {
+            bool free_slot = false;
+            for (const auto &sl : S->slots)
+                free_slot = free_slot || !sl.busy;
+            return scheduler_has_work(!S->finished.empty(), S->stop, S->inflight, !S->pending.empty(),
+                                      S->pending.empty() ? 0 : S->pending.front()->bytes, S->used, S->budget,
+                                      free_slot);
+        });
+        // retire (the timings are read without the lock; a finished group's
+        // slot stays busy until it is retired, so its timing state is not
+        // reused meanwhile)
+        std::vector<Group *> done;
+        done.swap(S->finished);
+        if (!done.empty()) {
+            lk.unlock();
+            for (Group *G : done)
+                B::read_timings(S, G);
+            lk.lock();
+        }
+        for (Group *G : done) {
+            if (G->reqs.front()->t_submit >= S->t_window && G->timed) {
+                S->copy_in_ms_sum += G->ms[0];
+                S->kernel_ms_sum += G->ms[1];
+                S->copy_out_ms_sum += G->ms[2];
+                S->timed_groups++;
+            }
+            S->slots[(size_t)G->slot].busy = nullptr;
+            S->used -= G->bytes;
+            S->inflight -= (int32_t)G->reqs.size();
+            for (auto *r : G->reqs) {
+                r->state = kDone;
+                if (r->t_submit >= S->t_window) {
+                    S->completed++;
+                    S->lat_ms.push_back((r->t_done - r->t_submit) * 1e3);
+                    S->queue_ms_sum += (r->t_launch - r->t_submit) * 1e3;
+                    S->t_last = std::max(S->t_last, r->t_done);
+                }
+            }
+            delete G;
+        }
+        if (!done.empty())
+            S->cv_done.notify_all();
+        if (S->stop && S->pending.empty() && S->inflight == 0)
+            break;
+        // admit
+        while (!S->pending.empty()) {
+            int slot = -1;
+            for (size_t i = 0; i < S->slots.size(); i++)
+                if (!S->slots[i].busy) {
+                    slot = (int)i;
+                    break;
+                }
+            if (slot < 0)
+                break;
+            const std::vector<size_t> pick = pick_group(S->pending, S->used, S->budget, S->max_group, S->group_bytes);
+            if (pick.empty())
+                break;  // the head waits for memory
+            Group *G = new Group();
+            G->slot = slot;
+            for (size_t i : pick) {
+                auto *r = S->pending[i];
+                G->reqs.push_back(r);
+                G->bytes += r->bytes;
+                r->state = kRunning;
+            }
+            for (size_t k = pick.size(); k-- > 0;)  // back to front: earlier positions stay valid
+                S->pending.erase(S->pending.begin() + (std::ptrdiff_t)pick[k]);
+            S->used += G->bytes;
+            S->peak_used = std::max(S->peak_used, S->used);
+            S->inflight += (int32_t)G->reqs.size();
+            S->max_inflight = std::max(S->max_inflight, S->inflight);
+            S->max_group_seen = std::max(S->max_group_seen, (int32_t)G->reqs.size());
+            S->groups_launched++;
+            S->slots[(size_t)slot].busy = G;
+            const double t_launch = B::now();
+            for (auto *r : G->reqs)
+                r->t_launch = t_launch;
+            // launch without the lock: the completion of earlier groups must
+            // be able to report meanwhile
+            lk.unlock();
+            const auto st = B::launch(S, G);
+            if (st != 0)
+                B::release_failed(S, G);  // it never reaches group_finished
+            lk.lock();
+            if (st != 0) {
+                S->slots[(size_t)slot].busy = nullptr;
+                S->used -= G->bytes;
+                S->inflight -= (int32_t)G->reqs.size();
+                for (auto *r : G->reqs) {
+                    r->state = kFailed;
+                    r->status = st;
+                    S->failed++;
+                }
+                delete G;
+                S->cv_done.notify_all();
+            }
+        }
+    }
 }
 
 }  // namespace cola

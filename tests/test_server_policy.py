@@ -5,7 +5,10 @@ first, one (K, dtypes) key per group, the request-count, copy-byte and
 memory-budget caps, and no request left out that would have fitted when it was
 considered.  scheduler_has_work is checked over its whole truth table; in
 particular a head that does not fit in the budget must not count as work (the
-scheduler would spin holding the lock the completion callback needs)."""
+scheduler would spin holding the lock the completion callback needs).  And the
+scheduler loop itself (run_scheduler) runs against a fake device on CPU threads:
+every request ends, the budget and caps hold, failed launches and shutdown with
+work queued end cleanly, all within a deadline."""
 import os
 import subprocess
 
@@ -126,3 +129,48 @@ def test_scheduler_wake_condition(policy_exe):
     res = subprocess.run([policy_exe, "wake"], input="1\n0 0 1 1 600 500 1000 1\n", capture_output=True, text=True,
                          check=True)
     assert res.stdout.split() == ["0"]
+
+
+@pytest.fixture(scope="module")
+def sched_exe(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("sched") / "server_sched_main")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-pthread",
+                           "-I", os.path.join(REPO, "cola_b200", "csrc"),
+                           os.path.join(REPO, "tests", "server_sched_main.cpp"), "-o", exe])
+    return exe
+
+
+def run_sched(exe, scenario, seed):
+    # a scheduler that spins holding its lock never returns: the timeout ends it
+    res = subprocess.run([exe, scenario, str(seed)], capture_output=True, text=True, timeout=90)
+    assert res.returncode == 0, res.stdout + res.stderr
+    line = res.stdout.strip().splitlines()[-1]
+    assert line.startswith("ok "), line
+    return {k: int(v) for k, v in (kv.split("=") for kv in line.split()[1:])}
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_scheduler_loop_budget_one_at_a_time(sched_exe, seed):
+    c = run_sched(sched_exe, "budget", seed)
+    assert c["done"] == 400 and c["other"] == 0
+    assert c["max_inflight"] == 1 and c["peak"] <= c["budget"]
+    assert c["used"] == 0 and c["completed"] == 400
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_scheduler_loop_mixed_keys(sched_exe, seed):
+    c = run_sched(sched_exe, "mix", seed)
+    assert c["done"] == 400 and c["other"] == 0 and c["used"] == 0
+    assert c["max_inflight"] > 1 and c["max_group"] > 1 and c["groups"] < 400
+    assert c["max_group"] <= 8 and c["peak"] <= c["budget"]
+
+
+def test_scheduler_loop_failed_launches(sched_exe):
+    c = run_sched(sched_exe, "fail", 4)
+    assert c["failed"] > 0 and c["done"] + c["failed"] == 400 and c["other"] == 0
+    assert c["sfailed"] == c["failed"] and c["used"] == 0
+
+
+def test_scheduler_loop_shutdown_with_work_queued(sched_exe):
+    c = run_sched(sched_exe, "stop", 5)
+    assert c["done"] + c["cancelled"] == 300 and c["other"] == 0 and c["used"] == 0
