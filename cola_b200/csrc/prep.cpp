@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -523,6 +524,96 @@ cola_status validate_partition(const cola_partition_set &s, const PartHost &P)
     for (int64_t i = 0; i < nzr; i++)
         COLA_REQUIRE(P.r_rowIdx[(size_t)i] >= 0 && P.r_rowIdx[(size_t)i] < rows, COLA_ERROR_INVALID_ARGUMENT,
                      "partition %d: remote row id %d out of range", P.part, P.r_rowIdx[(size_t)i]);
+    return COLA_SUCCESS;
+}
+
+cola_status build_row_view(const cola_partition_set &s, int64_t hub_threshold, int64_t hub_segment,
+                           int64_t task_entries, RowView &rv)
+{
+    COLA_REQUIRE(hub_threshold >= 1 && hub_segment >= 1 && task_entries >= 1, COLA_ERROR_INVALID_ARGUMENT,
+                 "row view: hub_threshold, hub_segment and task_entries must be >= 1");
+    const int64_t N = s.num_nodes;
+    const int32_t P = s.nparts;
+    rv = RowView();
+    rv.ptr.assign((size_t)N + 1, 0);
+    for (const PartHost &ph : s.parts) {
+        for (size_t i = 0; i < ph.l_rowIdx.size(); i++)
+            rv.ptr[(size_t)(ph.row_lb + ph.l_rowIdx[i]) + 1] += ph.l_rowPtr[i + 1] - ph.l_rowPtr[i];
+        for (int32_t r : ph.r_rowIdx)
+            rv.ptr[(size_t)(ph.row_lb + r) + 1] += 1;
+    }
+    for (int64_t r = 0; r < N; r++)
+        rv.ptr[(size_t)r + 1] += rv.ptr[(size_t)r];
+    rv.col.resize((size_t)rv.ptr[(size_t)N]);
+    rv.val.resize((size_t)rv.ptr[(size_t)N]);
+    std::vector<int64_t> cur(rv.ptr.begin(), rv.ptr.end() - 1);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int32_t p = 0; p < P; p++) {
+        const PartHost &ph = s.parts[(size_t)p];
+        const int64_t clb = (int64_t)p * s.npp;
+        size_t ci = 0;
+        // the remote columns below `limit`, column by column (each column's
+        // rows are distinct, so every row receives its entries in column order)
+        auto remote_cols_below = [&](int64_t limit) {
+            for (; ci < ph.r_colIdx.size() && ph.r_colIdx[ci] < limit; ci++)
+                for (int32_t q = ph.r_colPtr[ci]; q < ph.r_colPtr[ci + 1]; q++) {
+                    const int64_t row = ph.row_lb + ph.r_rowIdx[(size_t)q];
+                    const int64_t at = cur[(size_t)row]++;
+                    rv.col[(size_t)at] = ph.r_colIdx[ci];
+                    rv.val[(size_t)at] = ph.r_val[(size_t)q];
+                }
+        };
+        remote_cols_below(clb);
+        for (size_t i = 0; i < ph.l_rowIdx.size(); i++) {
+            const int64_t row = ph.row_lb + ph.l_rowIdx[i];
+            for (int32_t q = ph.l_rowPtr[i]; q < ph.l_rowPtr[i + 1]; q++) {
+                const int64_t at = cur[(size_t)row]++;
+                rv.col[(size_t)at] = (int32_t)(clb + ph.l_colIdx[(size_t)q]);
+                rv.val[(size_t)at] = ph.l_val[(size_t)q];
+            }
+        }
+        remote_cols_below(INT64_MAX);
+    }
+    // hub rows -> fixed-length segments
+    for (int64_t r = 0; r < N; r++) {
+        const int64_t b = rv.ptr[(size_t)r], e = rv.ptr[(size_t)r + 1];
+        if (e - b <= hub_threshold)
+            continue;
+        rv.hub_row.push_back((int32_t)r);
+        rv.hub_seg.push_back((int64_t)rv.seg_row.size());
+        for (int64_t q = b; q < e; q += hub_segment) {
+            rv.seg_row.push_back((int32_t)r);
+            rv.seg_beg.push_back(q);
+        }
+    }
+    rv.hub_seg.push_back((int64_t)rv.seg_row.size());
+    // row blocks of about task_entries entries, never containing a hub row
+    int64_t start = -1, cost = 0;
+    for (int64_t r = 0; r < N; r++) {
+        const int64_t len = rv.ptr[(size_t)r + 1] - rv.ptr[(size_t)r];
+        if (len > hub_threshold) {
+            if (start >= 0) {
+                rv.task_rb.push_back((int32_t)start);
+                rv.task_re.push_back((int32_t)r);
+            }
+            start = -1;
+            cost = 0;
+            continue;
+        }
+        if (start < 0)
+            start = r;
+        cost += len + 2;
+        if (cost >= task_entries) {
+            rv.task_rb.push_back((int32_t)start);
+            rv.task_re.push_back((int32_t)(r + 1));
+            start = -1;
+            cost = 0;
+        }
+    }
+    if (start >= 0) {
+        rv.task_rb.push_back((int32_t)start);
+        rv.task_re.push_back((int32_t)N);
+    }
     return COLA_SUCCESS;
 }
 

@@ -64,6 +64,23 @@ cola_status workgroup_cols(int32_t N, int64_t nnz, const int32_t *row, const int
                            int32_t gs, int32_t stage, std::vector<int32_t> &out);
 cola_status validate_partition(const cola_partition_set &s, const PartHost &P);
 
+// The row-major view the default schedule runs on: for every output row its
+// entries in ascending global column order (the partition's remote columns
+// left of its own block, its local entries, the remote columns right of it),
+// rows longer than hub_threshold cut into hub_segment-entry segments, and the
+// other rows packed greedily into tasks of about task_entries (a row costs its
+// entries + 2; a task never spans a hub row).
+struct RowView {
+    std::vector<int64_t> ptr;  // N + 1
+    std::vector<int32_t> col;
+    std::vector<float> val;
+    std::vector<int32_t> seg_row, hub_row;  // segment -> its row; hub -> its row
+    std::vector<int64_t> seg_beg, hub_seg;  // segment -> first entry; hub -> first segment (nhub + 1)
+    std::vector<int32_t> task_rb, task_re;  // task -> rows [rb, re)
+};
+cola_status build_row_view(const cola_partition_set &s, int64_t hub_threshold, int64_t hub_segment,
+                           int64_t task_entries, RowView &rv);
+
 }  // namespace cola
 
 struct cola_partition_set {

@@ -735,101 +735,18 @@ cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *o
                                   g->tables[(size_t)p]));
     }
 
-    // row-major view: per output row, its remote entries left of the
-    // partition's own columns, its local entries, then the remote entries to
-    // the right -- i.e. ascending global column order
+    // row-major view (build_row_view in prep.cpp): per output row its
+    // entries in ascending global column order, hub segments, row tasks
     const bool rows = !(opts && opts->no_row_view);
-    std::vector<int64_t> rv_ptr;
-    std::vector<int32_t> rv_col, seg_row, hub_row;
-    std::vector<float> rv_val;
-    std::vector<int64_t> seg_beg, hub_seg;
-    std::vector<int32_t> task_rb, task_re;
+    RowView rv;
     if (rows) {
-        const int64_t N = g->N;
         g->hub_threshold = opts && opts->hub_threshold > 0 ? opts->hub_threshold : 256;
         g->hub_segment = opts && opts->hub_segment > 0 ? opts->hub_segment : 256;
-        rv_ptr.assign((size_t)N + 1, 0);
-        for (const PartHost &ph : ps->parts) {
-            for (size_t i = 0; i < ph.l_rowIdx.size(); i++)
-                rv_ptr[(size_t)(ph.row_lb + ph.l_rowIdx[i]) + 1] += ph.l_rowPtr[i + 1] - ph.l_rowPtr[i];
-            for (int32_t r : ph.r_rowIdx)
-                rv_ptr[(size_t)(ph.row_lb + r) + 1] += 1;
-        }
-        for (int64_t r = 0; r < N; r++)
-            rv_ptr[(size_t)r + 1] += rv_ptr[(size_t)r];
-        rv_col.resize((size_t)rv_ptr[(size_t)N]);
-        rv_val.resize((size_t)rv_ptr[(size_t)N]);
-        std::vector<int64_t> cur(rv_ptr.begin(), rv_ptr.end() - 1);
-#pragma omp parallel for schedule(dynamic, 1)
-        for (int32_t p = 0; p < P; p++) {
-            const PartHost &ph = ps->parts[(size_t)p];
-            const int64_t clb = (int64_t)p * ps->npp;
-            size_t ci = 0;
-            auto remote_cols_below = [&](int64_t limit) {
-                for (; ci < ph.r_colIdx.size() && ph.r_colIdx[ci] < limit; ci++)
-                    for (int32_t q = ph.r_colPtr[ci]; q < ph.r_colPtr[ci + 1]; q++) {
-                        const int64_t row = ph.row_lb + ph.r_rowIdx[(size_t)q];
-                        const int64_t at = cur[(size_t)row]++;
-                        rv_col[(size_t)at] = ph.r_colIdx[ci];
-                        rv_val[(size_t)at] = ph.r_val[(size_t)q];
-                    }
-            };
-            remote_cols_below(clb);
-            for (size_t i = 0; i < ph.l_rowIdx.size(); i++) {
-                const int64_t row = ph.row_lb + ph.l_rowIdx[i];
-                for (int32_t q = ph.l_rowPtr[i]; q < ph.l_rowPtr[i + 1]; q++) {
-                    const int64_t at = cur[(size_t)row]++;
-                    rv_col[(size_t)at] = (int32_t)(clb + ph.l_colIdx[(size_t)q]);
-                    rv_val[(size_t)at] = ph.l_val[(size_t)q];
-                }
-            }
-            remote_cols_below(INT64_MAX);
-        }
-        // hub rows -> fixed-length segments
-        for (int64_t r = 0; r < N; r++) {
-            const int64_t b = rv_ptr[(size_t)r], e = rv_ptr[(size_t)r + 1];
-            if (e - b <= g->hub_threshold)
-                continue;
-            hub_row.push_back((int32_t)r);
-            hub_seg.push_back((int64_t)seg_row.size());
-            for (int64_t q = b; q < e; q += g->hub_segment) {
-                seg_row.push_back((int32_t)r);
-                seg_beg.push_back(q);
-            }
-        }
-        hub_seg.push_back((int64_t)seg_row.size());
-        g->nseg = (int64_t)seg_row.size();
-        g->nhub = (int64_t)hub_row.size();
-        // row blocks of about task_entries entries (a row costs its entries
-        // plus 2 for its write), never containing a hub row
         g->task_entries = opts && opts->task_entries > 0 ? opts->task_entries : 128;
-        int64_t start = -1, cost = 0;
-        for (int64_t r = 0; r < N; r++) {
-            const int64_t len = rv_ptr[(size_t)r + 1] - rv_ptr[(size_t)r];
-            if (len > g->hub_threshold) {
-                if (start >= 0) {
-                    task_rb.push_back((int32_t)start);
-                    task_re.push_back((int32_t)r);
-                }
-                start = -1;
-                cost = 0;
-                continue;
-            }
-            if (start < 0)
-                start = r;
-            cost += len + 2;
-            if (cost >= g->task_entries) {
-                task_rb.push_back((int32_t)start);
-                task_re.push_back((int32_t)(r + 1));
-                start = -1;
-                cost = 0;
-            }
-        }
-        if (start >= 0) {
-            task_rb.push_back((int32_t)start);
-            task_re.push_back((int32_t)N);
-        }
-        g->ntask = (int64_t)task_rb.size();
+        COLA_TRY(build_row_view(*ps, g->hub_threshold, g->hub_segment, g->task_entries, rv));
+        g->nseg = (int64_t)rv.seg_row.size();
+        g->nhub = (int64_t)rv.hub_row.size();
+        g->ntask = (int64_t)rv.task_rb.size();
     }
 
     // one device allocation for everything
@@ -880,15 +797,15 @@ cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *o
     size_t o_rv_ptr = 0, o_rv_col = 0, o_rv_val = 0, o_seg_row = 0, o_seg_beg = 0, o_hub_row = 0, o_hub_seg = 0;
     size_t o_task_rb = 0, o_task_re = 0;
     if (rows) {
-        o_rv_ptr = ar.add(rv_ptr.data(), rv_ptr.size() * 8);
-        o_rv_col = ar.add(rv_col.data(), rv_col.size() * 4);
-        o_rv_val = ar.add(rv_val.data(), rv_val.size() * 4);
-        o_seg_row = ar.add(seg_row.data(), seg_row.size() * 4);
-        o_seg_beg = ar.add(seg_beg.data(), seg_beg.size() * 8);
-        o_hub_row = ar.add(hub_row.data(), hub_row.size() * 4);
-        o_hub_seg = ar.add(hub_seg.data(), hub_seg.size() * 8);
-        o_task_rb = ar.add(task_rb.data(), task_rb.size() * 4);
-        o_task_re = ar.add(task_re.data(), task_re.size() * 4);
+        o_rv_ptr = ar.add(rv.ptr.data(), rv.ptr.size() * 8);
+        o_rv_col = ar.add(rv.col.data(), rv.col.size() * 4);
+        o_rv_val = ar.add(rv.val.data(), rv.val.size() * 4);
+        o_seg_row = ar.add(rv.seg_row.data(), rv.seg_row.size() * 4);
+        o_seg_beg = ar.add(rv.seg_beg.data(), rv.seg_beg.size() * 8);
+        o_hub_row = ar.add(rv.hub_row.data(), rv.hub_row.size() * 4);
+        o_hub_seg = ar.add(rv.hub_seg.data(), rv.hub_seg.size() * 8);
+        o_task_rb = ar.add(rv.task_rb.data(), rv.task_rb.size() * 4);
+        o_task_re = ar.add(rv.task_re.data(), rv.task_re.size() * 4);
     }
     ar.total = std::max<size_t>(ar.total, 256);
     COLA_CUDA(cudaMalloc(&g->dmem, ar.total));
