@@ -16,6 +16,7 @@
 #include "graph.h"
 #include "batch.h"
 #include "spmm_batch.cuh"
+#include "tune_cache.h"
 
 using cola::dev::BatchGraph;
 
@@ -470,35 +471,25 @@ cola_status cola_batch_autotune_cached(cola_batch *b, int32_t reps, const char *
                  "cola_batch_autotune_cached: bind the dense operands first");
     COLA_REQUIRE(cache_path, COLA_ERROR_INVALID_ARGUMENT, "cola_batch_autotune_cached: cache path is NULL");
     const std::string key = cola::tune_key(b);
-    if (FILE *f = std::fopen(cache_path, "r")) {
-        char line[1024];
-        while (std::fgets(line, sizeof line, f)) {
-            char k[600];
-            int u = 0, gp = 0, bps = 0;
-            float ms = 0.f;
-            if (std::sscanf(line, "%599s %d %d %d %f", k, &u, &gp, &bps, &ms) == 5 && key == k &&
-                (u == 2 || u == 4) && gp >= 10 && gp <= 100 && (bps == 3 || bps == 4)) {
-                std::fclose(f);
-                b->unroll = u;
-                b->grid_pct = gp;
-                b->blocks_per_sm = bps;
-                if (best_ms)
-                    *best_ms = ms;
-                if (from_cache)
-                    *from_cache = 1;
-                return COLA_SUCCESS;
-            }
-        }
-        std::fclose(f);
+    TuneEntry e;
+    if (tune_cache_find(cache_path, key, e)) {
+        b->unroll = e.unroll;
+        b->grid_pct = e.grid_pct;
+        b->blocks_per_sm = e.blocks_per_sm;
+        if (best_ms)
+            *best_ms = e.ms;
+        if (from_cache)
+            *from_cache = 1;
+        return COLA_SUCCESS;
     }
     float ms = 0.f;
     COLA_TRY(cola_batch_autotune(b, reps, stream, &ms));
-    FILE *f = std::fopen(cache_path, "a");
-    COLA_REQUIRE(f, COLA_ERROR_IO, "cola_batch_autotune_cached: cannot append to %s", cache_path);
-    std::fprintf(f, "%s %d %d %d %.6f\n", key.c_str(), b->unroll, b->grid_pct, b->blocks_per_sm, ms);
-    const bool werr = std::ferror(f) != 0;
-    std::fclose(f);
-    COLA_REQUIRE(!werr, COLA_ERROR_IO, "cola_batch_autotune_cached: cannot write %s", cache_path);
+    e.unroll = b->unroll;
+    e.grid_pct = b->grid_pct;
+    e.blocks_per_sm = b->blocks_per_sm;
+    e.ms = ms;
+    COLA_REQUIRE(tune_cache_append(cache_path, key, e), COLA_ERROR_IO,
+                 "cola_batch_autotune_cached: cannot append to %s", cache_path);
     if (best_ms)
         *best_ms = ms;
     if (from_cache)
