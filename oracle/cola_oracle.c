@@ -466,6 +466,84 @@ void orc_spmm_csr_f64(int64_t nrows, const int32_t *rowPtr, const int32_t *colId
     }
 }
 
+/*
+ * FP32 SpMM in one fixed order, to be matched bit for bit: row by row,
+ * entries in CSR order, one fused multiply-add (fmaf, correctly rounded) per
+ * product into an accumulator that starts at +0.  A row with more than
+ * hub_threshold entries is summed as segments of hub_segment entries (each
+ * from +0); the segment partials are then added by a binary counter -- partial
+ * s is added onto the open block sums of sizes 1, 2, 4, ... that the trailing
+ * one bits of s close -- and the open sums are folded largest first.  This is
+ * the summation order of cola_b200's row-major schedule for row tiles of one
+ * warp (32 lanes x 16 bytes: K a multiple of 128 with FP32 X); the math is the
+ * reference's SpMM (include/utils.cuh:45-69, SAG_reference_host) with values.
+ */
+int orc_spmm_rows_f32_ordered(int64_t nrows, const int64_t *rowPtr, const int32_t *colIdx, const float *val,
+                              const float *X, int64_t ldx, int32_t K, int64_t hub_threshold, int64_t hub_segment,
+                              float *Y, int64_t ldy)
+{
+    if (hub_threshold < 1 || hub_segment < 1 || K < 1)
+        return ORC_ERR;
+    int bad = 0;
+#pragma omp parallel
+    {
+        float *stk = (float *)malloc((size_t)65 * K * sizeof(float));  /* levels 0..63, then a partial */
+        if (!stk) {
+#pragma omp atomic write
+            bad = 1;
+        }
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t i = 0; i < nrows; i++) {
+            if (!stk)
+                continue;
+            float *y = Y + i * ldy;
+            const int64_t b = rowPtr[i], e = rowPtr[i + 1];
+            if (e - b <= hub_threshold) {
+                for (int32_t k = 0; k < K; k++)
+                    y[k] = 0.0f;
+                for (int64_t p = b; p < e; p++) {
+                    const float v = val[p];
+                    const float *x = X + (int64_t)colIdx[p] * ldx;
+                    for (int32_t k = 0; k < K; k++)
+                        y[k] = fmaf(v, x[k], y[k]);
+                }
+                continue;
+            }
+            const int64_t m = (e - b + hub_segment - 1) / hub_segment;
+            float *c = stk + (size_t)64 * K;
+            for (int64_t sgi = 0; sgi < m; sgi++) {
+                const int64_t q1 = b + (sgi + 1) * hub_segment < e ? b + (sgi + 1) * hub_segment : e;
+                for (int32_t k = 0; k < K; k++)
+                    c[k] = 0.0f;
+                for (int64_t p = b + sgi * hub_segment; p < q1; p++) {
+                    const float v = val[p];
+                    const float *x = X + (int64_t)colIdx[p] * ldx;
+                    for (int32_t k = 0; k < K; k++)
+                        c[k] = fmaf(v, x[k], c[k]);
+                }
+                int l = 0;
+                while ((sgi >> l) & 1) {
+                    const float *a = stk + (size_t)l * K;
+                    for (int32_t k = 0; k < K; k++)
+                        c[k] = a[k] + c[k];
+                    l++;
+                }
+                memcpy(stk + (size_t)l * K, c, (size_t)K * sizeof(float));
+            }
+            int first = 1;
+            for (int l = 63; l >= 0; l--)
+                if ((m >> l) & 1) {
+                    const float *a = stk + (size_t)l * K;
+                    for (int32_t k = 0; k < K; k++)
+                        y[k] = first ? a[k] : y[k] + a[k];
+                    first = 0;
+                }
+        }
+        free(stk);
+    }
+    return bad ? ORC_ERR : ORC_OK;
+}
+
 /* Same with BF16 X (raw uint16 bit patterns, widened exactly to FP32). */
 void orc_spmm_csr_f64_bf16x(int64_t nrows, const int32_t *rowPtr, const int32_t *colIdx,
                             const float *val, const uint16_t *X, int64_t ldx, int32_t K,

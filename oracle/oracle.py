@@ -42,6 +42,7 @@ def lib():
         L.orc_stage_tables.argtypes = [I32, I32, I32, I32, P, I64, I64, P, P, P, P, P, P, P, I64, P, P, I64]
         L.orc_spmm_csr_f64.argtypes = [I64, P, P, P, P, I64, I32, P, I64]
         L.orc_spmm_csr_f64_bf16x.argtypes = [I64, P, P, P, P, I64, I32, P, I64]
+        L.orc_spmm_rows_f32_ordered.argtypes = [I64, P, P, P, P, I64, I32, I64, I64, P, I64]
         L.orc_spmm_partition_f64.argtypes = [I32, I32, P, P, P, P, I64, P, P, P, P, I64, P, I64, I32, P, I64]
         L.orc_spmm_partitions_f32_omp.argtypes = [I32, I32] + [P] * 15 + [I64, I32, P, I64, I32]
         L.orc_max_threads.restype = I32
@@ -214,6 +215,25 @@ def spmm_csr_f64(rowPtr, colIdx, val, X):
         L.orc_spmm_csr_f64_bf16x(nrows, _ptr(rowPtr), _ptr(colIdx), _ptr(val), _ptr(X), X.shape[1], K, _ptr(Y), K)
     else:
         raise TypeError(X.dtype)
+    return Y
+
+
+def spmm_rows_f32_ordered(rowPtr, colIdx, val, X, hub_threshold=256, hub_segment=256):
+    """FP32 Y = A X summed in the row-major schedule's fixed order (fused
+    multiply-adds in CSR order per row; rows over hub_threshold entries as
+    hub_segment-entry segments added by a binary counter), to be compared bit
+    for bit.  X float32 (n x K)."""
+    L = lib()
+    nrows = len(rowPtr) - 1
+    X = np.ascontiguousarray(X, np.float32)
+    K = X.shape[1]
+    Y = np.zeros((nrows, K), np.float32)
+    rowPtr = np.ascontiguousarray(rowPtr, np.int64)
+    colIdx = np.ascontiguousarray(colIdx, np.int32)
+    val = np.ascontiguousarray(val, np.float32)
+    if L.orc_spmm_rows_f32_ordered(nrows, _ptr(rowPtr), _ptr(colIdx), _ptr(val), _ptr(X), K, K,
+                                   int(hub_threshold), int(hub_segment), _ptr(Y), K) != 0:
+        raise RuntimeError("orc_spmm_rows_f32_ordered failed")
     return Y
 
 

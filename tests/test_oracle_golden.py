@@ -80,3 +80,19 @@ def test_openmp_partition_loop_matches_fp64():
     rp, ci, vv = oracle.global_csr(n, row, col, val)
     ref = oracle.spmm_csr_f64(rp, ci, vv, X)
     assert oracle.rel_frobenius(Y[:n], ref) <= 1e-5
+
+
+def test_ordered_fp32_restatement_against_fp64():
+    """orc_spmm_rows_f32_ordered (the row-major schedule's summation order,
+    compared bit for bit with the GPU in test_zz_rows_order_gpu.py) computes the
+    FP64 oracle's product to FP32 accuracy for every hub setting, and the same
+    bits on every call."""
+    import cola_b200 as cb
+    n, row, col, val = cb.rmat(11, 16, seed=4)
+    rp, ci, vv = oracle.global_csr(n, row, col, val)
+    X = np.random.Generator(np.random.Philox(2)).standard_normal((n, 128), dtype=np.float32)
+    ref = oracle.spmm_csr_f64(rp, ci, vv, X)
+    for thr, seg in ((256, 256), (16, 8), (1, 1), (10 ** 6, 256)):
+        Y = oracle.spmm_rows_f32_ordered(rp, ci, vv, X, thr, seg)
+        assert np.linalg.norm(Y - ref) / np.linalg.norm(ref) < 1e-6
+        assert np.array_equal(Y, oracle.spmm_rows_f32_ordered(rp, ci, vv, X, thr, seg))
