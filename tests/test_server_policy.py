@@ -174,3 +174,19 @@ def test_scheduler_loop_failed_launches(sched_exe):
 def test_scheduler_loop_shutdown_with_work_queued(sched_exe):
     c = run_sched(sched_exe, "stop", 5)
     assert c["done"] + c["cancelled"] == 300 and c["other"] == 0 and c["used"] == 0
+
+
+def test_scheduler_loop_has_no_data_race(tmp_path):
+    """The same runs under ThreadSanitizer: no data race between the scheduler,
+    the submitting thread and the completion reports."""
+    exe = str(tmp_path / "server_sched_tsan")
+    build = subprocess.run(["g++", "-O1", "-g", "-std=c++17", "-fsanitize=thread", "-pthread",
+                            "-I", os.path.join(REPO, "cola_b200", "csrc"),
+                            os.path.join(REPO, "tests", "server_sched_main.cpp"), "-o", exe],
+                           capture_output=True, text=True)
+    if build.returncode != 0:
+        pytest.skip("ThreadSanitizer unavailable: " + build.stderr.strip().splitlines()[-1])
+    for scenario in ("budget", "fail", "stop"):
+        res = subprocess.run([exe, scenario, "9"], capture_output=True, text=True, timeout=300)
+        assert "ThreadSanitizer" not in res.stderr, res.stderr[:4000]
+        assert res.returncode == 0 and res.stdout.startswith("ok "), res.stdout + res.stderr[:2000]
