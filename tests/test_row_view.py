@@ -135,3 +135,34 @@ def test_row_view_rejects_bad_options(row_view_exe, tmp_path):
     with pytest.raises(subprocess.CalledProcessError) as e:
         build(row_view_exe, tmp_path, n, row, col, val, 2, 0, 256, 128)
     assert e.value.returncode == 4
+
+
+def test_host_builders_clean_under_address_and_ub_sanitizers(tmp_path):
+    """The partition build and the row view (host C++ with OpenMP) run clean
+    under AddressSanitizer and UndefinedBehaviorSanitizer on power-law, random
+    and mostly-empty inputs."""
+    exe = str(tmp_path / "row_view_asan")
+    build_cmd = ["g++", "-O1", "-g", "-std=c++17", "-fopenmp", "-fsanitize=address,undefined",
+                 "-fno-omit-frame-pointer", "-I", os.path.join(REPO, "include"),
+                 "-I", os.path.join(REPO, "cola_b200", "csrc"), "-I", "/usr/local/cuda/include",
+                 os.path.join(REPO, "tests", "row_view_main.cpp"),
+                 os.path.join(REPO, "cola_b200", "csrc", "prep.cpp"), "-o", exe]
+    res = subprocess.run(build_cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        pytest.skip("sanitizers unavailable: " + res.stderr.strip().splitlines()[-1])
+    n1, r1, c1, v1 = cb.rmat(11, 16, seed=5)
+    r2, c2, v2 = random_coo(1001, 300, seed=7)
+    for (n, row, col, val), P, thr, seg, te in (((n1, r1, c1, v1), 4, 256, 256, 128),
+                                                  ((n1, r1, c1, v1), 3, 1, 1, 1),
+                                                  ((1001, r2, c2, v2), 8, 4, 2, 16)):
+        inp, out = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+        with open(inp, "wb") as f:
+            np.array([n, P], np.int32).tofile(f)
+            np.array([len(row), thr, seg, te], np.int64).tofile(f)
+            np.asarray(row, np.int32).tofile(f)
+            np.asarray(col, np.int32).tofile(f)
+            np.asarray(val, np.float32).tofile(f)
+        run = subprocess.run([exe, inp, out], capture_output=True, text=True, timeout=300,
+                             env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1", UBSAN_OPTIONS="halt_on_error=1"))
+        assert run.returncode == 0 and "runtime error" not in run.stderr and "ERROR" not in run.stderr, \
+            run.stderr[:4000]
