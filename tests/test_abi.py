@@ -4,6 +4,7 @@ import ctypes
 import os
 import re
 import subprocess
+import sys
 
 import cola_b200
 from cola_b200 import _lib
@@ -42,3 +43,21 @@ def test_status_strings_and_version():
     assert L.cola_status_string(0) == b"success"
     assert L.cola_status_string(6) == b"over memory budget"
     assert b"sm_100a" in L.cola_version()
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """Without the native library every entry point raises: there is no CPU
+    fallback behind the package."""
+    import os
+    import sys
+    code = ("import cola_b200._lib as L\n"
+            "L.LIB_PATH = {!r}\n"
+            "import cola_b200 as cb\n"
+            "try:\n"
+            "    cb.PartitionSet.from_coo(4, [0, 1], [1, 2], [1.0, 1.0], 2)\n"
+            "except RuntimeError as e:\n"
+            "    print('raised:', e)\n").format(str(tmp_path / "absent.so"))
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=repo, timeout=300)
+    assert res.returncode == 0, res.stderr
+    assert "raised: cola_b200 native library missing" in res.stdout
