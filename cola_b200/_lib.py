@@ -66,7 +66,7 @@ class ZipView(ctypes.Structure):
 
 class SpmmOpts(ctypes.Structure):
     _fields_ = [("accumulate", I32), ("schedule", I32), ("gather_batch_rows", I32), ("unroll", I32),
-                ("min_blocks", I32), ("reserved", I32 * 3)]
+                ("min_blocks", I32), ("k_tile", I32), ("reserved", I32 * 2)]
 
 
 class BatchInfo(ctypes.Structure):
@@ -101,6 +101,7 @@ SIGNATURES = {
     "cola_nnz_split": (I32, [P, I64, P, I64, P, P, I64, P]),
     "cola_partition_build_device": (I32, [I32, I64, P, P, P, I32, P, P]),
     "cola_set_gather_bulk": (I32, [I32]),
+    "cola_set_gather_wait_limit": (I32, [I64]),
     "cola_device_error_check": (I32, [P]),
     "cola_graph_build_device": (I32, [I32, I64, P, P, P, I32, P, P, P]),
     "cola_nnz_split_device": (I32, [P, I64, P, I64, P, P, I64, P, P]),

@@ -185,6 +185,7 @@ static int *device_error_flag()
 }
 
 static std::atomic<int> g_gather_bulk{0};  // off: the vector gather measured as fast or faster
+static std::atomic<uint32_t> g_gather_wait_limit{dev::kWaitLimitDefault};
 
 // Bulk-copy (TMA) gather, when switched on, for rows of 1 KB or more (measured
 // alone: within 1 % of the vector gather from 1 KB to 4 KB, behind below 1 KB;
@@ -231,7 +232,8 @@ static bool launch_gather_bulk(const GatherSeg *segs, const GatherSeg &single, i
     const int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(ns, per_warp));
     t_launches++;
     fn<<<(unsigned)gx, dev::kThreads, smem, st>>>(segs, single, nsegs, total, static_cast<const T *>(src), ld_src,
-                                                  static_cast<T *>(dst), ld_dst, K, ns, chunk, slot, err);
+                                                  static_cast<T *>(dst), ld_dst, K, ns, chunk, slot,
+                                                  g_gather_wait_limit.load(), err);
     const cudaError_t e = cudaGetLastError();
     rc = e == cudaSuccess ? COLA_SUCCESS : fail(COLA_ERROR_CUDA, "gather (bulk copies): %s", cudaGetErrorString(e));
     return true;
@@ -293,6 +295,7 @@ struct RowsLaunch {
     int accumulate;
     int unroll;
     int min_blocks;
+    int k_tile;
 };
 
 template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC>
@@ -363,13 +366,34 @@ static cola_status launch_block_t(const dev::BlockArgs &ba, const RowsLaunch &a,
     using T = typename dev::ElemOf<TR>::T;
     constexpr int W = LG * NV * TR::E;
     auto fn = dev::rowblock_spmm_kernel<TR, TY, LG, NV, UNROLL, VEC, MINB>;
-    const int64_t gx = grid_for((const void *)fn, ba.nseg + ba.ntask);
-    const int gy = (a.K + W - 1) / W;
+    // one grid sweeps the feature tiles one after another
+    const int64_t ntile = (a.K + W - 1) / W;
+    const int64_t gx = grid_for((const void *)fn, (ba.nseg + ba.ntask) * ntile);
     t_launches++;
-    fn<<<dim3((unsigned)gx, (unsigned)gy), dev::kThreads, 0, st>>>(ba, static_cast<const T *>(a.X), a.ldx,
-                                                                   static_cast<TY *>(a.Y), a.ldy, a.K, a.accumulate);
+    fn<<<(unsigned)gx, dev::kThreads, 0, st>>>(ba, static_cast<const T *>(a.X), a.ldx, static_cast<TY *>(a.Y), a.ldy,
+                                               a.K, a.accumulate);
     COLA_CUDA(cudaGetLastError());
     return COLA_SUCCESS;
+}
+
+// Narrow passes (a full warp on a 64- or 128-feature tile, 8 or 4 bytes per
+// lane): loads in flight 4 or 8, resident blocks per SM 4, 6 or 8.
+template <typename TR, typename TY>
+static cola_status launch_block_narrow(const dev::BlockArgs &ba, const RowsLaunch &a, cudaStream_t st)
+{
+    const int mb = a.min_blocks == 6 || a.min_blocks == 8 ? a.min_blocks : 4;
+    if (a.unroll == 8) {
+        if (mb == 8)
+            return launch_block_t<TR, TY, 32, 1, 8, true, 8>(ba, a, st);
+        if (mb == 6)
+            return launch_block_t<TR, TY, 32, 1, 8, true, 6>(ba, a, st);
+        return launch_block_t<TR, TY, 32, 1, 8, true, 4>(ba, a, st);
+    }
+    if (mb == 8)
+        return launch_block_t<TR, TY, 32, 1, 4, true, 8>(ba, a, st);
+    if (mb == 6)
+        return launch_block_t<TR, TY, 32, 1, 4, true, 6>(ba, a, st);
+    return launch_block_t<TR, TY, 32, 1, 4, true, 4>(ba, a, st);
 }
 
 // V = 16-byte vectors per row: LG lanes per row tile, G = 32/LG lane groups.
@@ -412,12 +436,46 @@ static cola_status launch_block_geo(const dev::BlockArgs &ba, const RowsLaunch &
     return launch_block_t<TR, TY, 32, 4, 2, true>(ba, a, st);
 }
 
+// Feature tile of one pass for the requested k_tile (0 = the library's
+// choice), in the regime where a full warp covers one tile (K >= 128 FP32 X,
+// K >= 256 BF16 X); 0 where k_tile does not apply.
+static int rows_k_tile(cola_dtype xdt, int K, int k_tile)
+{
+    const int e16 = xdt == COLA_FLOAT32 ? 4 : 8;
+    if (K < 32 * e16 || k_tile <= 0)
+        return 0;
+    if (xdt == COLA_FLOAT32)
+        return k_tile == 64 || k_tile == 128 || k_tile == 256 || k_tile == 512 ? k_tile : 0;
+    return k_tile == 64 || k_tile == 128 || k_tile == 256 || k_tile == 512 || k_tile == 1024 ? k_tile : 0;
+}
+
 // Row-block streaming launch (vector path).
 static cola_status launch_block(const dev::BlockArgs &ba, const RowsLaunch &a, cudaStream_t st)
 {
     if (ba.nseg + ba.ntask <= 0)
         return COLA_SUCCESS;
     using BF = __nv_bfloat16;
+    const int kt = rows_k_tile(a.xdt, a.K, a.k_tile);
+    if (kt > 0) {
+        // every tile width sums each element in the same order (one lane group)
+        const int e16 = a.xdt == COLA_FLOAT32 ? 4 : 8;
+        if (a.xdt == COLA_FLOAT32 && kt == 64)
+            return a.ydt == COLA_FLOAT32 ? launch_block_narrow<dev::NarrowTraits<float, 8>, float>(ba, a, st)
+                                         : launch_block_narrow<dev::NarrowTraits<float, 8>, BF>(ba, a, st);
+        if (a.xdt == COLA_BFLOAT16 && kt == 128)
+            return a.ydt == COLA_FLOAT32 ? launch_block_narrow<dev::NarrowTraits<BF, 8>, float>(ba, a, st)
+                                         : launch_block_narrow<dev::NarrowTraits<BF, 8>, BF>(ba, a, st);
+        if (a.xdt == COLA_BFLOAT16 && kt == 64)
+            return a.ydt == COLA_FLOAT32 ? launch_block_narrow<dev::NarrowTraits<BF, 4>, float>(ba, a, st)
+                                         : launch_block_narrow<dev::NarrowTraits<BF, 4>, BF>(ba, a, st);
+        // 16-byte vectors, NV per lane: V = kt / e16 selects the geometry below
+        const int V = kt / e16;
+        if (a.xdt == COLA_FLOAT32)
+            return a.ydt == COLA_FLOAT32 ? launch_block_geo<dev::VecTraits<float>, float>(ba, a, V, st)
+                                         : launch_block_geo<dev::VecTraits<float>, BF>(ba, a, V, st);
+        return a.ydt == COLA_FLOAT32 ? launch_block_geo<dev::VecTraits<BF>, float>(ba, a, V, st)
+                                     : launch_block_geo<dev::VecTraits<BF>, BF>(ba, a, V, st);
+    }
     if (a.xdt == COLA_FLOAT32)
         return a.ydt == COLA_FLOAT32 ? launch_block_geo<dev::VecTraits<float>, float>(ba, a, a.K / 4, st)
                                      : launch_block_geo<dev::VecTraits<float>, BF>(ba, a, a.K / 4, st);
@@ -1015,6 +1073,15 @@ cola_status cola_set_gather_bulk(int32_t enable)
     return COLA_SUCCESS;
 }
 
+cola_status cola_set_gather_wait_limit(int64_t polls)
+{
+    COLA_REQUIRE(polls >= 0 && polls <= (int64_t)dev::kWaitLimitDefault * 64, COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_set_gather_wait_limit: polls=%lld (0 .. %lld)", (long long)polls,
+                 (long long)dev::kWaitLimitDefault * 64);
+    g_gather_wait_limit.store(polls == 0 ? dev::kWaitLimitDefault : (uint32_t)polls);
+    return COLA_SUCCESS;
+}
+
 cola_status cola_graph_zip_view(const cola_graph *g, int32_t part, cola_zip_view *o)
 {
     COLA_REQUIRE(g && o && part >= 0 && part < g->P, COLA_ERROR_INVALID_ARGUMENT,
@@ -1097,6 +1164,7 @@ static cola_status spmm_impl(cola_graph *g, const void *X, cola_dtype xdt, int64
         a.accumulate = accumulate;
         a.unroll = opts ? opts->unroll : 0;
         a.min_blocks = opts ? opts->min_blocks : 0;
+        a.k_tile = opts ? opts->k_tile : 0;
         if (a.vec) {
             dev::BlockArgs ba;
             ba.rowptr = g->rv_ptr;

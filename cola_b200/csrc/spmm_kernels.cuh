@@ -87,6 +87,58 @@ struct VecTraits<__nv_bfloat16> {
     }
 };
 
+// Narrower vectors (BYTES = 8 or 4 per lane) for feature tiles a full warp
+// reads 256 or 128 bytes of: the row-major schedule's narrow passes.
+template <typename T, int BYTES>
+struct NarrowTraits;
+
+template <>
+struct NarrowTraits<float, 8> {
+    static constexpr int E = 2;
+    using raw_t = float2;
+    __device__ __forceinline__ static raw_t load(const float *p) { return __ldg(reinterpret_cast<const float2 *>(p)); }
+    __device__ __forceinline__ static raw_t zero() { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ static void unpack(const raw_t &r, float (&f)[E])
+    {
+        f[0] = r.x;
+        f[1] = r.y;
+    }
+};
+
+template <>
+struct NarrowTraits<__nv_bfloat16, 8> {
+    static constexpr int E = 4;
+    using raw_t = uint2;
+    __device__ __forceinline__ static raw_t load(const __nv_bfloat16 *p)
+    {
+        return __ldg(reinterpret_cast<const uint2 *>(p));
+    }
+    __device__ __forceinline__ static raw_t zero() { return make_uint2(0u, 0u); }
+    __device__ __forceinline__ static void unpack(const raw_t &r, float (&f)[E])
+    {
+        f[0] = __uint_as_float(r.x << 16);
+        f[1] = __uint_as_float(r.x & 0xffff0000u);
+        f[2] = __uint_as_float(r.y << 16);
+        f[3] = __uint_as_float(r.y & 0xffff0000u);
+    }
+};
+
+template <>
+struct NarrowTraits<__nv_bfloat16, 4> {
+    static constexpr int E = 2;
+    using raw_t = uint32_t;
+    __device__ __forceinline__ static raw_t load(const __nv_bfloat16 *p)
+    {
+        return __ldg(reinterpret_cast<const unsigned int *>(p));
+    }
+    __device__ __forceinline__ static raw_t zero() { return 0u; }
+    __device__ __forceinline__ static void unpack(const raw_t &r, float (&f)[E])
+    {
+        f[0] = __uint_as_float(r << 16);
+        f[1] = __uint_as_float(r & 0xffff0000u);
+    }
+};
+
 // Scalar fallback (rows not 16-byte aligned or K not a multiple of E).
 template <typename T>
 struct ScalarTraits {
@@ -109,6 +161,10 @@ struct ElemOf<VecTraits<__nv_bfloat16>> {
 };
 template <typename U>
 struct ElemOf<ScalarTraits<U>> {
+    using T = U;
+};
+template <typename U, int B>
+struct ElemOf<NarrowTraits<U, B>> {
     using T = U;
 };
 
@@ -309,26 +365,34 @@ struct GatherSeg {
 // issues every row's load at once, stores each row as its load lands on the
 // slot's mbarrier, and waits for the stores to finish reading before the next
 // chunk reuses the slots.  Rows are K elements of 16-byte granularity, every
-// address 16-byte aligned (checked by the host).  Every wait is bounded: past
-// the limit the kernel records an error in *err, drains its own copies (again
-// bounded) and stops.
+// address 16-byte aligned (checked by the host).  Every wait is bounded.  A
+// row's wait gives up after `wait_limit` polls (a kernel argument); the kernel
+// then records error 1 in *err, stops issuing copies and drains every load it
+// has issued, each with the separate, much larger kDrainLimit, before the CTA
+// exits (its bulk stores are waited for by cp.async.bulk.wait_group, which
+// always ends).  Only if a drain wait also runs out is error 2 recorded: a load
+// may then still be writing this CTA's shared memory after it exits.
 // ---------------------------------------------------------------------------
 constexpr int kGatherMaxSlots = 32;
-constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr uint32_t kWaitLimitDefault = 1u << 22;  // polls: at least 0.25 s
+constexpr uint32_t kDrainLimit = 1u << 25;        // polls: at least 2 s
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
+// Polls the mbarrier's phase `parity` up to `limit` times (non-blocking
+// test_wait, a short sleep between polls); true once the phase completed.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32_t limit)
 {
-    for (uint32_t i = 0; i < kWaitLimit; i++) {
+    for (uint32_t i = 0; i < limit; i++) {
         uint32_t done;
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(done)
             : "r"(mbar), "r"(parity)
             : "memory");
         if (done)
             return true;
+        __nanosleep(64);
     }
     return false;
 }
@@ -362,7 +426,8 @@ __global__ void __launch_bounds__(kThreads) gather_rows_bulk_kernel(const Gather
                                                                     int nsegs, int64_t total,
                                                                     const T *__restrict__ src, int64_t ld_src,
                                                                     T *__restrict__ dst, int64_t ld_dst, int K,
-                                                                    int ns, int chunk, int slot_bytes, int *err)
+                                                                    int ns, int chunk, int slot_bytes,
+                                                                    uint32_t wait_limit, int *err)
 {
     extern __shared__ __align__(128) unsigned char s_dyn[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -403,7 +468,7 @@ __global__ void __launch_bounds__(kThreads) gather_rows_bulk_kernel(const Gather
         for (int j = 0; j < cnt; j++) {  // each row's store as its load lands
             T *d_j = reinterpret_cast<T *>(__shfl_sync(kFull, reinterpret_cast<uintptr_t>(dp), j));
             if (lane == 0 && ok) {
-                if (!mbar_wait(bar0 + 8u * j, (phase >> j) & 1u)) {
+                if (!mbar_wait(bar0 + 8u * j, (phase >> j) & 1u, wait_limit)) {
                     ok = 0;
                     pending_from = j;
                     pending_to = cnt;
@@ -424,10 +489,13 @@ __global__ void __launch_bounds__(kThreads) gather_rows_bulk_kernel(const Gather
     }
     if (lane == 0) {
         if (!ok) {
-            atomicExch(err, 1);
-            for (int j = pending_from; j < pending_to; j++)  // drain the loads still in flight (bounded)
-                if (!mbar_wait(bar0 + 8u * j, (phase >> j) & 1u))
-                    break;
+            // every load issued for rows pending_from .. pending_to-1 lands
+            // before the CTA exits (no store is issued for them)
+            int code = 1;
+            for (int j = pending_from; j < pending_to; j++)
+                if (!mbar_wait(bar0 + 8u * j, (phase >> j) & 1u, kDrainLimit))
+                    code = 2;
+            atomicMax(err, code);
         }
         asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
     }

@@ -64,6 +64,24 @@ __device__ __forceinline__ void store_out<__nv_bfloat16, 4, true>(__nv_bfloat16 
 }
 
 template <>
+__device__ __forceinline__ void store_out<float, 2, true>(float *p, const float (&a)[2], bool accumulate)
+{
+    float2 v = make_float2(a[0], a[1]);
+    if (accumulate) {
+        const float2 o = *reinterpret_cast<const float2 *>(p);
+        v.x += o.x;
+        v.y += o.y;
+    }
+    __stcs(reinterpret_cast<float2 *>(p), v);
+}
+
+template <>
+__device__ __forceinline__ void store_out<__nv_bfloat16, 2, true>(__nv_bfloat16 *p, const float (&a)[2], bool)
+{
+    *reinterpret_cast<uint32_t *>(p) = pack_bf16x2(a[0], a[1]);
+}
+
+template <>
 __device__ __forceinline__ void store_out<float, 1, false>(float *p, const float (&a)[1], bool accumulate)
 {
     *p = accumulate ? *p + a[0] : a[0];
@@ -452,11 +470,24 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
     __shared__ int2 s_ent[kWarpsPerBlock][32];
     int2 *ent = s_ent[threadIdx.x >> 5];
     constexpr int W = LG * NV * TR::E;
-    const int k0 = blockIdx.y * W;
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    const int64_t w0 = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     const int64_t total = ba.nseg + ba.ntask;
-    rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5),
-                                                  nwarps, total, X, ldx, Y, ldy, K, accumulate, k0, ent);
+    const int ntile = (K + W - 1) / W;
+    if (ntile == 1) {
+        rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, w0, nwarps, total, X, ldx, Y, ldy, K, accumulate, 0, ent);
+        return;
+    }
+    // Feature tiles one after another: the grid sweeps every item of tile 0,
+    // then of tile 1, ..., so the X columns being gathered at any moment are
+    // one tile wide (a smaller working set in L2).  Every element's sum is the
+    // same chain of FMAs whichever tile width computes it.
+    for (int64_t w = w0; w < total * ntile; w += nwarps) {
+        const int tile = (int)(w / total);
+        const int64_t it = w - (int64_t)tile * total;
+        rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, it, 1, it + 1, X, ldx, Y, ldy, K, accumulate, tile * W,
+                                                      ent);
+    }
 }
 
 // Hub rows: sum the segment partials ws[s0 .. s1) pairwise — a binary tree in

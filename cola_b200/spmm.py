@@ -100,9 +100,11 @@ class Graph:
         return z
 
     def spmm(self, X, Y=None, out_dtype=None, accumulate=False, schedule=SCHEDULE_AUTO, gather_batch_rows=0,
-             unroll=0, min_blocks=0, stream=None):
+             unroll=0, min_blocks=0, k_tile=0, stream=None):
         """Y = A X (Y += A X with accumulate).  X: (>= N) x K CUDA tensor,
-        float32 or bfloat16; Y: N x K float32 or bfloat16 (allocated when None)."""
+        float32 or bfloat16; Y: N x K float32 or bfloat16 (allocated when None).
+        unroll, min_blocks and k_tile tune the row-major schedule (0 = the
+        library's choice; every choice gives the same bits)."""
         _dense(X, "X")
         K = X.shape[1]
         if X.shape[0] < self.num_nodes:
@@ -118,6 +120,7 @@ class Graph:
         o.gather_batch_rows = int(gather_batch_rows)
         o.unroll = int(unroll)
         o.min_blocks = int(min_blocks)
+        o.k_tile = int(k_tile)
         check(lib().cola_spmm(self._h, _ptr(X), _DT[X.dtype], X.stride(0), _ptr(Y), _DT[Y.dtype], Y.stride(0), K,
                               ctypes.byref(o), _stream(stream)))
         return Y

@@ -328,8 +328,20 @@ cola_status cola_graph_get_info(const cola_graph *g, cola_graph_info *out);
  * way; on a B200 the vector gather measured as fast or faster. */
 cola_status cola_set_gather_bulk(int32_t enable);
 
+/* How many times the bulk-copy gather polls for one row's load before it gives
+ * up (0 = the default, 4,194,304 polls: at least a quarter of a second).  A
+ * wait that gives up makes that launch stop early and drain the loads it
+ * issued; cola_device_error_check then reports it.  Small values exist to
+ * exercise that path. */
+cola_status cola_set_gather_wait_limit(int64_t polls);
+
 /* Waits for the current device, then reports (and clears) the error code a
- * kernel left when one of its bounded waits ran out: 0 = none. */
+ * kernel left when one of its bounded waits ran out: 0 = none; 1 = a bulk-copy
+ * gather stopped early (it drained every copy it had issued before exiting);
+ * 2 = as 1, and a drain also ran out (a copy may have still been in flight when
+ * its block exited).  Any nonzero code means that the results of every launch
+ * on the device since the previous check must not be used; after code 2 the
+ * device should not be trusted for further work in this process. */
 cola_status cola_device_error_check(int32_t *code);
 
 /* Device pointers of partition `part`'s split arrays (the d_csr_zip / d_csc_zip
@@ -362,7 +374,11 @@ typedef struct cola_spmm_opts {
     int32_t unroll;             /* ROWS: row loads in flight per lane group (2, 4, 6 or 8; 0 = 4) */
     int32_t min_blocks;         /* ROWS: resident blocks per SM the kernel is compiled for (3, 4, 5, 6;
                                    0 = 3 for FP32 X, 4 for BF16 X) */
-    int32_t reserved[3];
+    int32_t k_tile;             /* ROWS, K >= 128 (FP32 X) or >= 256 (BF16 X): features per pass over the
+                                   graph (64, 128, 256, 512, 1024; 0 = chosen by the library).  The passes
+                                   run one after another so the X columns in use are one tile wide; every
+                                   choice gives the same bits.  Ignored for narrower K. */
+    int32_t reserved[2];
 } cola_spmm_opts;
 
 /* Y = A X (or Y += A X) for all partitions.  X: >= P*npp rows (rows past N are

@@ -499,3 +499,33 @@ def test_bulk_gather_schedules(case12, K, xdt):
     ref = fp64_reference(n, row, col, val, X.float().cpu().numpy())
     assert rel(outs[1][0].cpu().numpy(), ref) <= TOL_F32
     assert rel(outs[1][1].cpu().numpy(), ref) <= TOL_F32
+
+
+def test_bulk_gather_wait_limit_reports_and_drains():
+    """A bulk-copy gather whose per-row wait is cut to one poll gives up on
+    its first row, reports error 1 (it stopped early and drained every load it
+    had issued: no copy is left in flight), and the device stays usable: with
+    the default limit the same gather is exact again and reports nothing."""
+    npp, P, nemb, K = 4096, 4, 20000, 1024  # 4 KB rows, far slower than one poll
+    X = torch.from_numpy(dense_x(P * npp, K, seed=5)).to(DEV)
+    rng = np.random.Generator(np.random.Philox(5))
+    idx = torch.from_numpy(rng.integers(0, P * npp, nemb).astype(np.int32)).to(DEV)
+    want = X[(idx.long() % npp)]
+    out = torch.zeros((nemb, K), device=DEV)
+    assert _device_error() == 0
+    try:
+        assert cb.lib().cola_set_gather_bulk(1) == 0
+        assert cb.lib().cola_set_gather_wait_limit(1) == 0
+        cb._lib.check(cb.lib().cola_batching_data_ppl(ptr(X), ptr(out), ptr(idx), nemb, K, npp, 1, None))
+        torch.cuda.synchronize()
+        assert _device_error() == 1
+        assert cb.lib().cola_set_gather_wait_limit(0) == 0
+        out.zero_()
+        cb._lib.check(cb.lib().cola_batching_data_ppl(ptr(X), ptr(out), ptr(idx), nemb, K, npp, 1, None))
+        torch.cuda.synchronize()
+        assert _device_error() == 0
+        assert torch.equal(out, want)
+    finally:
+        cb.lib().cola_set_gather_wait_limit(0)
+        cb.lib().cola_set_gather_bulk(0)
+    assert cb.lib().cola_set_gather_wait_limit(-1) == 1  # COLA_ERROR_INVALID_ARGUMENT
