@@ -1,16 +1,22 @@
 """Benchmark of the partitioned SpMM on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload fp32|bf16]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload bf16|fp32|...]
 
-Default workload: R-MAT scale 20 (1,048,576 nodes), avg degree 32, symmetrised,
-values D^-1/2 A D^-1/2, P = 8 virtual row partitions, X 1,048,576 x 128 FP32
-~N(0,1) (Philox, seed 2), FP32 output.  A step is one Y = A X over all
-partitions, inputs resident in HBM (default schedule: the row-major view, one
-writer per output row; --schedule fused runs the CSC-scatter kernel).  The
-metric is algorithmic HBM GB/s:
+Default workload (the precision form): R-MAT scale 21 (2,097,152 nodes), avg
+degree 48, symmetrised, values D^-1/2 A D^-1/2, P = 8 virtual row partitions,
+X 2,097,152 x 256 stored BF16 (rounded from FP32 ~N(0,1), Philox seed 3), FP32
+accumulation, BF16 output.  A step is one Y = A X over all partitions, inputs
+resident in HBM (default schedule: the row-major view, one writer per output
+row).  The metric is algorithmic HBM GB/s:
     B = nnz*(4 + s_v + K*s_x) + (M+1)*4 + M*K*s_y   (s_v = 4)
-per step divided by the step time.  Inputs (X 512 MiB, Y 512 MiB) are larger
-than L2, so no L2 flush runs between timed steps.
+per step divided by the step time.  Inputs (X and Y 1 GiB each) are larger than
+L2, so no L2 flush runs between timed steps.  At one GPU the same line also
+carries the plain FP32 path on the identical graph (fp32_same_graph, with the
+BF16 speed-up), configuration 2 (R-MAT scale 20, K = 128, FP32) beside the
+reference's own CUDA kernels (fp32_config2), and the serving loop's p50/p99
+(serving).  roofline.frac is physical: DRAM bytes per SpMM from the committed
+ncu summary of the same build, over the kernels' time (alg_frac beside it is
+the per-nonzero model above).
 
 Multi-GPU (torchrun): every rank runs an independent replica of the workload
 on its own GPU (replicas only: the single-GPU path has no exchange between
@@ -191,16 +197,18 @@ def dense_x(n, K, seed):
     return g.standard_normal((n, K), dtype=np.float32)
 
 
-def fp64_error(n, row, col, val, Xh, Y, dev, samples=4096):
+def fp64_error(n, row, col, val, Xh, Y, dev, samples=4096, longest=64):
     """Relative Frobenius error of Y on a row sample (evenly spaced rows plus
-    the 16 longest rows) against Y = A X computed in FP64 on the GPU from the
-    FP32 features -- FP64 is used only in this validation reduction."""
+    the `longest` rows with the most entries, where a power-law graph's hubs
+    are) against Y = A X computed in FP64 on the GPU from the FP32 features --
+    FP64 is used only in this validation reduction.  Returns (error, rows
+    sampled, entries of the longest sampled row)."""
     import torch
     counts = np.bincount(row, minlength=n)
     rowptr = np.zeros(n + 1, np.int64)
     np.cumsum(counts, out=rowptr[1:])
     pick = np.unique(np.concatenate([np.linspace(0, n - 1, samples).astype(np.int64),
-                                     np.argsort(counts)[-16:].astype(np.int64)]))
+                                     np.argsort(counts, kind="stable")[-longest:].astype(np.int64)]))
     crow = [0]
     cols, vals = [], []
     for r in pick:
@@ -220,22 +228,48 @@ def fp64_error(n, row, col, val, Xh, Y, dev, samples=4096):
     got = Y[torch.from_numpy(pick).to(dev)].double()
     err = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
     del X64
-    return err, int(len(pick))
+    return err, int(len(pick)), int(counts.max())
 
 
-def read_traffic(name):
-    """traffic_bytes_per_launch from a committed ncu summary, if any."""
+PROFILE_FILES = {"fp32": "spmm_dram_rmat20_k128_fp32.md", "bf16": "spmm_dram_rmat21_k256_bf16.md",
+                 "fp32-k256": "spmm_dram_rmat21_k256_fp32.md"}
+
+
+def read_profile(name):
+    """The `key = value` lines of a committed ncu summary under profiles/."""
     p = os.path.join(REPO, "profiles", name)
+    out = {}
     if not os.path.exists(p):
-        return None
+        return out
     with open(p) as f:
         for line in f:
-            if line.strip().startswith("traffic_bytes_per_launch"):
-                try:
-                    return int(float(line.split("=")[1].split()[0]))
-                except (IndexError, ValueError):
-                    return None
-    return None
+            t = line.strip()
+            if "=" in t and not t.startswith(("|", "#", "ncu", "python")):
+                k, v = t.split("=", 1)
+                out[k.strip()] = v.strip().split()[0] if v.strip() else ""
+    return out
+
+
+def profiled_traffic(workload, opts_key):
+    """DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one
+    SpMM (both of its launches) from the committed summary of this workload,
+    when that summary was taken on the native sources built now and with the
+    same launch options; else None.  Returns (bytes or None, why)."""
+    from cola_b200 import _build
+    name = PROFILE_FILES.get(workload)
+    if name is None:
+        return None, "no profile for this workload"
+    prof = read_profile(name)
+    if "traffic_bytes_per_spmm" not in prof:
+        return None, "profiles/{} absent".format(name)
+    have = _build.source_hash()
+    if prof.get("build_source_hash") != have:
+        return None, "profiles/{} was taken on sources {}, built now: {}".format(
+            name, prof.get("build_source_hash"), have)
+    if prof.get("launch_options", "") != opts_key:
+        return None, "profiles/{} was taken with options {}, this run: {}".format(
+            name, prof.get("launch_options"), opts_key)
+    return int(float(prof["traffic_bytes_per_spmm"])), "profiles/{} (sources {})".format(name, have)
 
 
 def measured_peak():
@@ -307,7 +341,9 @@ def run_reference(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    n, row, col, val = make_graph(w)
+    # the oracle's restatement of the generator: the same graph, bit for bit, with
+    # nothing of the product loaded in this process
+    n, row, col, val = oracle.rmat(w["scale"], w["deg"], w["seed"])
     rp, ci, _ = oracle.global_csr(n, row, col, val)
     K = w["K"]
     X = dense_x(n, K, w["seed"])
@@ -321,7 +357,7 @@ def run_reference(args, w):
         times.append(dt)
     t = sum(times) / len(times)
     s = 4 if w["xdt"] == "fp32" else 2
-    B = alg_bytes(nnz, rows, K, 4, 4)  # the reference computes in FP32
+    B = alg_bytes(nnz, rows, K, 4, 4)  # the bytes the reference moves: it computes in FP32
     v = B / t / 1e9
     sample = "{} threads x {} rows (rows spread over the matrix), {} of {} rows, {} nnz per step".format(
         nth, rows_per, rows, n, nnz)
@@ -334,6 +370,43 @@ def run_reference(args, w):
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def spmm_kw(args):
+    """Launch options of the row-major schedule given on the command line."""
+    return dict(unroll=args.unroll, min_blocks=args.min_blocks, k_tile=args.k_tile)
+
+
+def opts_key(args):
+    return "unroll={},min_blocks={},k_tile={}".format(args.unroll, args.min_blocks, args.k_tile)
+
+
+def time_steps(step, steps, warmup, stream):
+    """Average device time of `steps` calls of step() between two CUDA events
+    on `stream`, after `warmup` untimed calls, synchronised on both sides."""
+    import torch
+    for _ in range(max(warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    for _ in range(steps):
+        step()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    return ev[0].elapsed_time(ev[1]) / steps
+
+
+def time_each(step, runs, stream):
+    """Device time of each of `runs` calls (CUDA events around every call)."""
+    import torch
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(runs)]
+    for a, b in kev:
+        a.record(stream)
+        step()
+        b.record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in kev]
 
 
 def run_ours(args, w):
@@ -373,12 +446,10 @@ def run_ours(args, w):
              "rows": S.SCHEDULE_ROWS}[args.schedule]
     eff = S.SCHEDULE_ROWS if sched == S.SCHEDULE_AUTO else sched
     B = alg_bytes(int(info.nnz), n, K, s_x, s_y)
+    kw = spmm_kw(args)
 
     def step():
-        g.spmm(X, Y, schedule=sched, unroll=args.unroll, min_blocks=args.min_blocks, stream=stream)
-
-    def barrier():
-        world_barrier()
+        g.spmm(X, Y, schedule=sched, stream=stream, **kw)
 
     def max_over_ranks(x):
         return world_reduce(x, dev, "max")
@@ -386,7 +457,7 @@ def run_ours(args, w):
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()
-    barrier()
+    world_barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
     clocks.start()
@@ -396,7 +467,7 @@ def run_ours(args, w):
         step()
     ev[1].record(stream)
     torch.cuda.synchronize()
-    barrier()
+    world_barrier()
     torch.cuda.synchronize()
     ms = ev[0].elapsed_time(ev[1]) / args.steps
     ms = max_over_ranks(ms)
@@ -405,14 +476,8 @@ def run_ours(args, w):
     # launch without the Y zeroing); the row-major schedule has no zeroing
     Yacc = torch.zeros((n, K), dtype=torch.float32, device=dev) if eff == S.SCHEDULE_FUSED else Y
     # at least 50 launches, so that the median is taken over 50 or more runs
-    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(max(args.steps, 50))]
-    for a, b in kev:
-        a.record(stream)
-        g.spmm(X, Yacc, accumulate=(eff == S.SCHEDULE_FUSED), schedule=sched, unroll=args.unroll, min_blocks=args.min_blocks, stream=stream)
-        b.record(stream)
-    torch.cuda.synchronize()
-    k_list = [a.elapsed_time(b) for a, b in kev]
+    k_list = time_each(lambda: g.spmm(X, Yacc, accumulate=(eff == S.SCHEDULE_FUSED), schedule=sched, stream=stream,
+                                      **kw), max(args.steps, 50), stream)
     k_ms = max_over_ranks(sum(k_list) / len(k_list))
     k_med = max_over_ranks(statistics.median(k_list))
     clocks.hold(step)
@@ -434,7 +499,7 @@ def run_ours(args, w):
 
         def serial():
             Xd[0].copy_(Xpin[0], non_blocking=True)
-            g.spmm(Xd[0], Yd[0], schedule=sched, stream=stream)
+            g.spmm(Xd[0], Yd[0], schedule=sched, stream=stream, **kw)
             Ypin[0].copy_(Yd[0], non_blocking=True)
 
         s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
@@ -451,7 +516,7 @@ def run_ours(args, w):
                 ev["x_ready"][b].record(s_in)
             stream.wait_event(ev["x_ready"][b])
             stream.wait_event(ev["y_free"][b])
-            g.spmm(Xd[b], Yd[b], schedule=sched, stream=stream)
+            g.spmm(Xd[b], Yd[b], schedule=sched, stream=stream, **kw)
             ev["x_free"][b].record(stream)
             ev["y_ready"][b].record(stream)
             s_out.wait_event(ev["y_ready"][b])
@@ -462,7 +527,7 @@ def run_ours(args, w):
         for _ in range(2):
             serial()
         torch.cuda.synchronize()
-        barrier()
+        world_barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(e2e_steps):
@@ -473,7 +538,7 @@ def run_ours(args, w):
         for i in range(2):
             pipelined(i)
         torch.cuda.synchronize()
-        barrier()
+        world_barrier()
         e0.record(stream)
         for i in range(e2e_steps):
             pipelined(i)
@@ -481,18 +546,27 @@ def run_ours(args, w):
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
-        barrier()
+        world_barrier()
         # the pipelined results are the product too
         if not torch.equal(Ypin[(e2e_steps - 1) % 2], Yd[(e2e_steps - 1) % 2].cpu()):
             raise RuntimeError("pipelined e2e: host Y differs from the device result")
         Y.copy_(Yd[0])
+        del Xpin, Ypin, Xd, Yd
 
-    err, nsamp = fp64_error(n, row, col, val, Xh, Y, dev)
+    err, nsamp, longest = fp64_error(n, row, col, val, Xh, Y, dev)
     peak, peak_kind = measured_peak()
-    achieved = B / (k_ms * 1e-3) / 1e9
-    traffic = read_traffic({"fp32": "rowblock_spmm_rmat20_k128_fp32.md", "bf16": "rowblock_spmm_rmat21_k256_bf16.md",
-                            "fp32-k256": "rowblock_spmm_rmat21_k256_fp32.md"}[args.workload]) \
-        if eff == S.SCHEDULE_ROWS and args.scale is None and args.K is None else None
+    compulsory = int(info.nnz) * 8 + n * K * (s_x + s_y)
+    overridden = args.scale is not None or args.K is not None
+    if eff == S.SCHEDULE_ROWS and not overridden:
+        traffic, traffic_src = profiled_traffic(args.workload, opts_key(args))
+    else:
+        traffic, traffic_src = None, "no profile for this schedule or size"
+    k_s = k_ms * 1e-3
+    # physical: DRAM bytes ncu counted for this build / the kernels' time; without a
+    # profile of this build, the compulsory bytes (a lower bound of the traffic)
+    phys = traffic if traffic is not None else compulsory
+    achieved = phys / k_s / 1e9
+    alg_achieved = B / k_s / 1e9
     launches_per_step = int(g.get_info().last_launches)  # counted by the library
     line = {
         "metric": METRIC, "value": B * world / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world,
@@ -505,31 +579,57 @@ def run_ours(args, w):
                    "schedule": {S.SCHEDULE_ROWS: "rows", S.SCHEDULE_FUSED: "fused",
                                 S.SCHEDULE_BUFFER: "buffer"}.get(eff, args.schedule),
                    "hub_rows": int(info.hub_rows), "hub_segments": int(info.hub_segments),
-                   "unroll": args.unroll or 4, "row_tasks": int(info.row_tasks),
-                   "blocks_per_sm": args.min_blocks or (3 if xdt == torch.float32 else 4),
+                   "launch_options": opts_key(args), "row_tasks": int(info.row_tasks),
                    "alg_bytes_per_step": B,
                    "l2": "inputs larger than L2 (X {:.0f} MiB, Y {:.0f} MiB); no flush".format(
                        n * K * s_x / 2 ** 20, n * K * s_y / 2 ** 20),
                    "prep_seconds": round(t_prep, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_kind,
-                     "kernel_ms": k_ms, "kernel_ms_median": k_med, "kernel_runs": len(k_list), "frac_of_8TBs": achieved / 8000.0,
-                     # what must cross DRAM at least: indices and values once, X and Y once
-                     "compulsory_bytes": int(info.nnz) * 8 + n * K * (s_x + s_y),
-                     "traffic_over_compulsory": None if traffic is None else
-                     traffic / float(int(info.nnz) * 8 + n * K * (s_x + s_y))},
+                     "traffic": traffic,
+                     "frac_basis": ("DRAM bytes per SpMM counted by ncu on this build ({}) / the SpMM kernels' "
+                                    "time".format(traffic_src)) if traffic is not None else
+                                   ("compulsory bytes (indices and values once, X and Y once: a lower bound of the "
+                                    "DRAM traffic) / the SpMM kernels' time; traffic null: {}".format(traffic_src)),
+                     "peak_source": peak_kind,
+                     "kernel_ms": k_ms, "kernel_ms_median": k_med, "kernel_runs": len(k_list),
+                     "compulsory_bytes": compulsory,
+                     "traffic_over_compulsory": None if traffic is None else traffic / float(compulsory),
+                     # the per-nonzero row-gather model: one X row per entry, most of them L2 hits
+                     "alg_bytes": B, "alg_achieved": alg_achieved, "alg_frac": alg_achieved / peak,
+                     "alg_frac_of_8TBs": alg_achieved / 8000.0},
         "e2e": None if e2e_ms is None else {
             "value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": n * K * s_x,
             "d2h_bytes_per_step": n * K * s_y, "ms_per_step": e2e_ms,
             "mode": "pipelined: two steps in flight, step i+1's X upload overlapping step i's Y download",
             "serial_ms_per_step": e2e_serial_ms,
             "serial_value": B * world / (e2e_serial_ms * 1e-3) / 1e9},
-        "accuracy": {"rel_frobenius_vs_fp64": err, "rows_sampled": nsamp,
+        "accuracy": {"rel_frobenius_vs_fp64": err, "rows_sampled": nsamp, "longest_row_entries": longest,
                      "bound": 1e-5 if (xdt == torch.float32 and ydt == torch.float32) else 1e-2,
-                     "reference": "FP64 on the GPU from the FP32 features, sampled rows incl. the 16 longest"},
+                     "reference": "FP64 on the GPU from the FP32 features, 4,096 evenly spaced rows and the 64 "
+                                  "longest"},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
     }
+    extras = world == 1 and not args.no_extras and not overridden
+    if extras and xdt == torch.bfloat16:
+        # the plain FP32 path on the identical graph and features
+        X32 = torch.from_numpy(Xh).to(dev)
+        Y32 = torch.empty((n, K), dtype=torch.float32, device=dev)
+
+        def step32():
+            g.spmm(X32, Y32, schedule=sched, stream=stream, **kw)
+
+        ms32 = time_steps(step32, args.steps, args.warmup, stream)
+        k32 = time_each(step32, max(args.steps, 50), stream)
+        err32, _, _ = fp64_error(n, row, col, val, Xh, Y32, dev)
+        B32 = alg_bytes(int(info.nnz), n, K, 4, 4)
+        line["fp32_same_graph"] = {
+            "ms_per_step": ms32, "kernel_ms": sum(k32) / len(k32), "value": B32 / (ms32 * 1e-3) / 1e9,
+            "unit": "GB/s", "rel_frobenius_vs_fp64": err32, "bound": 1e-5,
+            "bf16_speedup": ms32 / ms, "bf16_kernel_speedup": (sum(k32) / len(k32)) / k_ms,
+            "note": "same graph, same X (FP32 features, FP32 output); bf16_speedup = FP32 step time / BF16 step "
+                    "time"}
+        del X32, Y32
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle
         rp, ci, vv = oracle.global_csr(n, row, col, val)
@@ -564,6 +664,7 @@ def run_ours(args, w):
             line["cpu_baseline"]["torch_sparse_mm"] = {
                 "value": alg_bytes(len(ci), n, K, 4, 4) / statistics.median(tt) / 1e9, "unit": "GB/s",
                 "cores": nth, "sample": "the whole matrix, FP32, median of 3"}
+            del A, Xc
         except (RuntimeError, MemoryError) as e:
             line["cpu_baseline"]["torch_sparse_mm"] = {"unavailable": str(e)[:200]}
         # and an OpenMP loop over the same P partitions (local CSR + remote CSC chunks)
@@ -571,12 +672,62 @@ def run_ours(args, w):
         # the reference's own CUDA kernels on this GPU (FP32 only, as the reference)
         if xdt == torch.float32 and ydt == torch.float32:
             line["reference_gpu_kernels"] = reference_kernels_baseline(g, X, n, K, w["P"], B, k_ms, stream)
+    g.close()
+    del X, Y, g, ps
+    torch.cuda.empty_cache()
+    if extras and args.workload == "bf16":
+        # the FP32 configuration the reference's kernels run (and the serving loop) in the same line
+        line["fp32_config2"] = fp32_config2_leg(args, stream)
+        torch.cuda.empty_cache()
+        if not args.no_serving:
+            line["serving"] = serving_leg(args, seconds=args.serve_seconds_default)[0]
     if rank == 0:
         print(json.dumps(line), flush=True)
-    g.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def fp32_config2_leg(args, stream):
+    """Configuration 2 (R-MAT scale 20, degree 32, K = 128, FP32, P = 8) on this
+    GPU: our step time, its FP64 error, and the reference's own CUDA kernels
+    on the same split blocks."""
+    import torch
+
+    import cola_b200 as cb
+    from cola_b200 import spmm as S
+    w = WORKLOADS["fp32"]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    n, row, col, val = make_graph(w)
+    ps = cb.PartitionSet.from_coo(n, row, col, val, w["P"])
+    K = w["K"]
+    Xh = dense_x(n, K, w["seed"])
+    g = S.Graph(ps, stream=stream)
+    X = torch.from_numpy(Xh).to(dev)
+    Y = torch.empty((n, K), device=dev)
+    kw = spmm_kw(args)
+
+    def step():
+        g.spmm(X, Y, stream=stream, **kw)
+
+    ms = time_steps(step, args.steps, args.warmup, stream)
+    kl = time_each(step, max(args.steps, 50), stream)
+    k_ms = sum(kl) / len(kl)
+    err, nsamp, _ = fp64_error(n, row, col, val, Xh, Y, dev)
+    B = alg_bytes(int(g.info.nnz), n, K, 4, 4)
+    compulsory = int(g.info.nnz) * 8 + n * K * 8
+    traffic, src = profiled_traffic("fp32", opts_key(args))
+    peak, _ = measured_peak()
+    out = {"workload": w["desc"], "nnz": int(g.info.nnz), "ms_per_step": ms, "kernel_ms": k_ms,
+           "value": B / (ms * 1e-3) / 1e9, "unit": "GB/s", "rel_frobenius_vs_fp64": err, "bound": 1e-5,
+           "rows_sampled": nsamp, "traffic": traffic, "traffic_source": src,
+           "frac": (traffic if traffic is not None else compulsory) / (k_ms * 1e-3) / 1e9 / peak,
+           "alg_frac": B / (k_ms * 1e-3) / 1e9 / peak}
+    if not args.no_cpu_baseline:
+        out["reference_gpu_kernels"] = reference_kernels_baseline(g, X, n, K, w["P"], B, k_ms, stream)
+    g.close()
+    del X, Y
+    return out
 
 
 def openmp_partitions_baseline(ps, Xh, K, P, nthreads):
@@ -856,22 +1007,17 @@ def run_batched(args):
     return 0
 
 
-def run_serving(args):
+def serving_leg(args, seconds):
+    """The serving workload: 64 resident graphs, a saturation burst, then an
+    open loop of Poisson arrivals at args.serve_load of the saturation rate for
+    `seconds`.  Returns the `serving` object of the bench line plus the served
+    bytes, wall time, request count and clocks."""
     import torch
 
     import cola_b200 as cb
     from cola_b200.serving import Server
 
-    if not torch.cuda.is_available():
-        raise RuntimeError("bench.py needs a CUDA device")
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", device_id=dev)
     t0 = time.time()
     rng = np.random.Generator(np.random.Philox(5))
     srv = Server(memory_budget=120 << 30, slots=4, max_group=16)
@@ -912,6 +1058,9 @@ def run_serving(args):
         sz = 4 if dt == torch.float32 else 2
         return alg_bytes(gnnz[g], gn[g], K, sz, sz)
 
+    def copy_bytes(g, K, dt):
+        return 2 * gn[g] * K * (4 if dt == torch.float32 else 2)
+
     # warm-up (single requests, then one untimed burst, which also grows the
     # server's memory pool to its working size), then the saturation rate: a
     # burst submitted at once
@@ -928,13 +1077,14 @@ def run_serving(args):
     cap = len(burst) / (time.perf_counter() - tb)
     # open loop: Poisson arrivals at a fraction of the saturation rate
     rate = args.serve_load * cap
-    nreq = max(args.serve_min_requests, int(rate * args.serve_seconds))
+    nreq = max(args.serve_min_requests, int(rate * seconds))
     srv.reset_stats()
     clocks = Clocks(local)
     clocks.start()
     plan = [draw() for _ in range(nreq)]
     gaps = rng.exponential(1.0 / rate, nreq)
     reqs = []
+    t_sub = []
     ts = time.perf_counter()
     t_next = ts
     for d, gap in zip(plan, gaps):
@@ -942,29 +1092,65 @@ def run_serving(args):
         delay = t_next - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
+        t_sub.append(time.perf_counter())
         reqs.append(submit(*d))
-    for r in reqs:
+    # per size class: latency from submission to the result in host memory,
+    # taken on this thread as each wait returns (waits in submission order, so
+    # a request's time is an upper bound when an earlier one finished later)
+    lat = [0.0] * nreq
+    for i, r in enumerate(reqs):
         r.wait(timeout_ms=WAIT_MS)
+        lat[i] = (time.perf_counter() - t_sub[i]) * 1e3
     wall = time.perf_counter() - ts
     clk = clocks.stop()
     st = srv.stats()
     B = sum(req_bytes(*d) for d in plan)
     h2d = sum(gn[g] * K * (4 if dt == torch.float32 else 2) for g, K, dt in plan) / nreq
+    classes = {}
+    for (gi, K, dt), ms_ in zip(plan, lat):
+        mb = copy_bytes(gi, K, dt) / 2 ** 20
+        c = "small (<16 MiB of copies)" if mb < 16 else ("medium (16-256 MiB)" if mb < 256 else "large (>=256 MiB)")
+        classes.setdefault(c, []).append(ms_)
+    per_class = {c: {"requests": len(v), "p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99))}
+                 for c, v in sorted(classes.items())}
+    srv.close()
+    return {"workload": SERVING_DESC, "graphs": len(gn), "nodes": int(sum(gn)), "nnz": int(sum(gnnz)),
+            "offered_req_per_s": rate, "saturation_req_per_s": cap, "achieved_req_per_s": st["req_per_s"],
+            "sustained": st["req_per_s"] >= 0.95 * rate,
+            "completed": st["completed"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "max_ms": st["max_ms"], "mean_ms": st["mean_ms"], "max_inflight": st["max_inflight"],
+            "groups_launched": st["groups_launched"], "max_group": st["max_group"],
+            "queue_ms_mean": st["queue_ms_mean"], "copy_in_ms_mean": st["copy_in_ms_mean"],
+            "kernel_ms_mean": st["kernel_ms_mean"], "copy_out_ms_mean": st["copy_out_ms_mean"],
+            "peak_device_bytes": st["peak_bytes"], "budget_bytes": st["budget"],
+            "per_size_class": per_class, "open_loop_seconds": round(wall, 2),
+            "served_GBps": B / wall / 1e9, "prep_seconds": round(t_prep, 1),
+            "latency": "submit to result in pinned host memory"}, B, wall, nreq, h2d, clk
+
+
+def run_serving(args):
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=dev)
+    serving, B, wall, nreq, h2d, clk = serving_leg(args, args.serve_seconds)
     value = world_reduce(B / wall / 1e9, dev, "sum")
     peak, peak_kind = measured_peak()
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": nreq,
             "warmup": max(args.warmup, 3), "ms_per_step": wall * 1e3 / nreq, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 and bf16-storage/f32-accum", "data": "synthetic",
-            "config": {"workload": SERVING_DESC, "graphs": len(gn), "nodes": int(sum(gn)), "nnz": int(sum(gnnz)),
-                       "parallelism": "replicas x{}".format(world), "prep_seconds": round(t_prep, 1)},
-            "serving": {"offered_req_per_s": rate, "saturation_req_per_s": cap, "achieved_req_per_s": st["req_per_s"],
-                        "completed": st["completed"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-                        "max_ms": st["max_ms"], "mean_ms": st["mean_ms"], "max_inflight": st["max_inflight"],
-                        "groups_launched": st["groups_launched"], "max_group": st["max_group"],
-                        "queue_ms_mean": st["queue_ms_mean"], "copy_in_ms_mean": st["copy_in_ms_mean"],
-                        "kernel_ms_mean": st["kernel_ms_mean"], "copy_out_ms_mean": st["copy_out_ms_mean"],
-                        "peak_device_bytes": st["peak_bytes"], "budget_bytes": st["budget"],
-                        "latency": "submit to result in pinned host memory"},
+            "config": {"workload": SERVING_DESC, "graphs": serving["graphs"], "nodes": serving["nodes"],
+                       "nnz": serving["nnz"], "parallelism": "replicas x{}".format(world),
+                       "prep_seconds": serving["prep_seconds"]},
+            "serving": serving,
             "roofline": {"bound": "hbm", "achieved": value / world, "peak": peak, "unit": "GB/s",
                          "frac": value / world / peak, "traffic": None,
                          "peak_source": peak_kind,
@@ -973,13 +1159,15 @@ def run_serving(args):
             "gpu_launches": None, "clocks": clk}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    srv.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
 
 
-def prep_case():
+def prep_case(oracle_gen=False):
+    if oracle_gen:  # the reference leg loads nothing of the product
+        from oracle import oracle
+        return oracle.rmat(20, 32, 2), 8
     import cola_b200 as cb
     return cb.rmat(20, 32, seed=2), 8
 
@@ -1006,7 +1194,7 @@ def run_prep_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    (n, row, col, val), P = prep_case()
+    (n, row, col, val), P = prep_case(oracle_gen=True)
     nth = min(host_threads(), P)
     for _ in range(max(args.warmup - 1, 0)):
         oracle_partitions(n, row, col, val, P, nth)
@@ -1152,7 +1340,7 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="fp32", choices=sorted(WORKLOADS) + ["batched", "serving", "prep"])
+    ap.add_argument("--workload", default="bf16", choices=sorted(WORKLOADS) + ["batched", "serving", "prep"])
     ap.add_argument("--serve-graphs", type=int, default=64)
     ap.add_argument("--serve-burst", type=int, default=64, help="serving: requests of the saturation burst")
     ap.add_argument("--serve-load", type=float, default=0.7, help="serving: offered rate / saturation rate")
@@ -1168,6 +1356,12 @@ def main():
     ap.add_argument("--unroll", type=int, default=0, help="row-major schedule: loads in flight per lane group")
     ap.add_argument("--task-entries", type=int, default=0, help="row-major schedule: entries per row-block task")
     ap.add_argument("--min-blocks", type=int, default=0, help="row-major schedule: resident blocks per SM")
+    ap.add_argument("--k-tile", type=int, default=0, help="row-major schedule: features per pass (0 = library's)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload: skip the FP32 same-graph, configuration-2 and serving legs")
+    ap.add_argument("--no-serving", action="store_true", help="default workload: skip the serving leg")
+    ap.add_argument("--serve-seconds-default", type=float, default=10.0,
+                    help="default workload: open-loop length of its serving leg")
     ap.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
     ap.add_argument("--K", type=int, default=None, help="override the feature width (exploration runs)")
     args = ap.parse_args()

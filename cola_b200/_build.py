@@ -42,6 +42,22 @@ def _headers():
         glob.glob(os.path.join(INCLUDE, "*.h"))
 
 
+def source_hash():
+    """16 hex digits identifying the native sources (csrc/ and include/): a
+    profile of the kernels records it, so a reader can tell whether the
+    profile was taken on the code that is built now."""
+    import hashlib
+    h = hashlib.sha256()
+    files = sorted(glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(INCLUDE, "*.h")) +
+                   glob.glob(os.path.join(INCLUDE, "cola", "*.h")))
+    for f in files:
+        if os.path.isfile(f):
+            h.update(os.path.relpath(f, REPO).encode())
+            with open(f, "rb") as fh:
+                h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
 def _stale(out, deps):
     if not os.path.exists(out):
         return True
@@ -91,4 +107,7 @@ def build(force=False, verbose=False):
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    if "--hash" in sys.argv:
+        print(source_hash())
+    else:
+        print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -77,7 +77,7 @@ class BatchInfo(ctypes.Structure):
 
 class ServerOpts(ctypes.Structure):
     _fields_ = [("memory_budget", I64), ("slots", I32), ("max_group", I32), ("group_mib", I32),
-                ("reserved", I32 * 3)]
+                ("small_mib", I32), ("copy_chunk_mib", I32), ("reserved", I32 * 1)]
 
 
 class ServerStats(ctypes.Structure):

@@ -74,6 +74,9 @@ struct cola_server {
     int64_t budget = 0, used = 0, peak_used = 0, graph_bytes = 0;
     int32_t max_group = 16;
     int64_t group_bytes = 32 << 20;
+    int64_t small_bytes = 16 << 20;  // size classes (server_policy.h); 0 = off
+    int32_t small_slots = 1;
+    int64_t copy_chunk = 32 << 20;
     std::vector<cola_graph *> graphs;
     std::vector<Slot> slots;
     // request buffers come from a pool of the server's own that keeps freed
@@ -106,6 +109,19 @@ struct HostCbArg {
     Group *g;
 };
 
+// One cudaMemcpyAsync per piece of at most `chunk` bytes: the copy engine
+// takes other streams' copies between the pieces, so a small request's copy
+// does not wait for the whole of a long one.
+static cola_status copy_chunked(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, int64_t chunk,
+                                cudaStream_t st)
+{
+    const size_t c = chunk > 0 ? (size_t)chunk : bytes;
+    for (size_t off = 0; off < bytes; off += c)
+        COLA_CUDA(cudaMemcpyAsync(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off,
+                                  std::min(c, bytes - off), kind, st));
+    return COLA_SUCCESS;
+}
+
 // Launch one admitted group on its slot: copy every X in, run one batched
 // launch over the group's graphs, copy every Y out, then signal completion.
 static cola_status launch_group(cola_server *S, Group *G)
@@ -125,7 +141,8 @@ static cola_status launch_group(cola_server *S, Group *G)
         COLA_CUDA(cudaMallocFromPoolAsync(&r->dY, (size_t)r->rows * r->K * ys, S->pool, st));
         if (g->nseg > 0)
             COLA_CUDA(cudaMallocFromPoolAsync((void **)&r->dws, (size_t)g->nseg * r->K * sizeof(float), S->pool, st));
-        COLA_CUDA(cudaMemcpyAsync(r->dX, r->X_host, (size_t)r->rows * r->K * xs, cudaMemcpyHostToDevice, st));
+        COLA_TRY(copy_chunked(r->dX, r->X_host, (size_t)r->rows * r->K * xs, cudaMemcpyHostToDevice,
+                              S->copy_chunk, st));
         BatchGraph &d = sl.h_desc[i];
         fill_batch_graph(d, g, r->dX, r->K, r->dY, r->K, r->K, r->xdt, r->dws);
         d.item0 = items;
@@ -149,7 +166,8 @@ static cola_status launch_group(cola_server *S, Group *G)
     COLA_TRY(launch_batch(L, st));
     COLA_CUDA(cudaEventRecord(sl.ev[2], st));
     for (Request *r : G->reqs)
-        COLA_CUDA(cudaMemcpyAsync(r->Y_host, r->dY, (size_t)r->rows * r->K * ys, cudaMemcpyDeviceToHost, st));
+        COLA_TRY(copy_chunked(r->Y_host, r->dY, (size_t)r->rows * r->K * ys, cudaMemcpyDeviceToHost,
+                              S->copy_chunk, st));
     COLA_CUDA(cudaEventRecord(sl.ev[3], st));
     for (Request *r : G->reqs) {
         COLA_CUDA(cudaFreeAsync(r->dX, st));
@@ -267,6 +285,8 @@ cola_status cola_server_create(const cola_server_opts *opts, cola_server **out)
     const int nslots = opts && opts->slots > 0 ? opts->slots : 4;
     S->max_group = opts && opts->max_group > 0 ? opts->max_group : 16;
     S->group_bytes = (int64_t)(opts && opts->group_mib > 0 ? opts->group_mib : 32) << 20;
+    S->small_bytes = opts && opts->small_mib < 0 ? 0 : (int64_t)(opts && opts->small_mib > 0 ? opts->small_mib : 16) << 20;
+    S->copy_chunk = (int64_t)(opts && opts->copy_chunk_mib > 0 ? opts->copy_chunk_mib : 32) << 20;
     cudaMemPoolProps pp;
     std::memset(&pp, 0, sizeof(pp));
     pp.allocType = cudaMemAllocationTypePinned;

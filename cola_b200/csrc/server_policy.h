@@ -11,6 +11,16 @@
 //     its head, however large),
 //   * the budget has room for the group with the request.
 // A request that does not fit is skipped, not dropped: it stays pending.
+//
+// Size classes (pick_admission): a request whose host<->device copies are at
+// most small_bytes is small, the others large.  A group holds one class only.
+// Small groups may take any free slot; large groups leave the last
+// small_slots slots to small ones.  When the head is large and no slot a large
+// group may take is free, the oldest small request opens a small group
+// instead, so that small requests are not held behind large copies; the
+// memory the head needs stays free for it (a small group passes only if the
+// head still fits beside it), so the head cannot be starved.  A head that
+// waits for memory is passed by nothing (memory is granted in queue order).
 #pragma once
 #include <algorithm>
 #include <condition_variable>
@@ -33,9 +43,39 @@ struct SchedGroup {
     int slot = 0;
     int64_t bytes = 0;
     bool completed = false;
+    bool small = false;  // opened by a small request (size classes)
     bool timed = false;
     float ms[3] = {0, 0, 0};  // copy-in, launch, copy-out (read when retired)
 };
+
+// The group opened by pending[first]: it and the later requests with its key
+// and, when small_bytes > 0, its size class, in queue order, under the count,
+// copy-byte and budget caps above.  Empty when pending[first] does not fit in
+// the budget.
+template <typename Seq>
+std::vector<size_t> scan_group(const Seq &pending, size_t first, int64_t used, int64_t budget, int32_t max_group,
+                               int64_t group_bytes, int64_t small_bytes)
+{
+    std::vector<size_t> out;
+    if (first >= pending.size())
+        return out;
+    const auto &head = *pending[first];
+    if (used + head.bytes > budget)
+        return out;
+    const bool head_small = head.copy_bytes <= small_bytes;
+    int64_t bytes = 0, copy = 0;
+    for (size_t i = first; i < pending.size() && (int32_t)out.size() < max_group && copy < group_bytes; i++) {
+        const auto &r = *pending[i];
+        if (r.K == head.K && r.xdt == head.xdt && r.ydt == head.ydt && used + bytes + r.bytes <= budget &&
+            (out.empty() || copy + r.copy_bytes <= group_bytes) &&
+            (small_bytes <= 0 || (r.copy_bytes <= small_bytes) == head_small)) {
+            out.push_back(i);
+            bytes += r.bytes;
+            copy += r.copy_bytes;
+        }
+    }
+    return out;
+}
 
 // R: any type with fields K, xdt, ydt (compared for equality), bytes (device
 // bytes while in flight) and copy_bytes (host <-> device bytes).  Returns the
@@ -45,39 +85,79 @@ template <typename Seq>
 std::vector<size_t> pick_group(const Seq &pending, int64_t used, int64_t budget, int32_t max_group,
                                int64_t group_bytes)
 {
-    std::vector<size_t> out;
-    if (pending.empty())
-        return out;
+    return scan_group(pending, 0, used, budget, max_group, group_bytes, 0);
+}
+
+struct Admission {
+    std::vector<size_t> pick;  // positions in `pending`, increasing
+    bool small = false;        // a small group (opened by a small request)
+};
+
+// The next group to admit under the size classes (header comment), or none.
+// slot_free: some slot is free; large_slot_free: a slot that a large group may
+// take is free.  small_bytes <= 0 turns the classes off (pick_group alone).
+template <typename Seq>
+Admission pick_admission(const Seq &pending, int64_t used, int64_t budget, int32_t max_group, int64_t group_bytes,
+                         int64_t small_bytes, bool slot_free, bool large_slot_free)
+{
+    Admission a;
+    if (pending.empty() || !slot_free)
+        return a;
     const auto &head = *pending[0];
     if (used + head.bytes > budget)
-        return out;
-    int64_t bytes = 0, copy = 0;
-    for (size_t i = 0; i < pending.size() && (int32_t)out.size() < max_group && copy < group_bytes; i++) {
-        const auto &r = *pending[i];
-        if (r.K == head.K && r.xdt == head.xdt && r.ydt == head.ydt && used + bytes + r.bytes <= budget &&
-            (out.empty() || copy + r.copy_bytes <= group_bytes)) {
-            out.push_back(i);
-            bytes += r.bytes;
-            copy += r.copy_bytes;
-        }
+        return a;  // the head waits for memory; nothing passes it
+    const bool head_small = small_bytes > 0 && head.copy_bytes <= small_bytes;
+    if (head_small || large_slot_free || small_bytes <= 0) {
+        a.pick = scan_group(pending, 0, used, budget, max_group, group_bytes, small_bytes);
+        a.small = head_small;
+        return a;
     }
-    return out;
+    // a large head waits for a slot: the oldest small request opens a small
+    // group in the memory left beside the head's
+    for (size_t i = 1; i < pending.size(); i++)
+        if (pending[i]->copy_bytes <= small_bytes) {
+            a.pick = scan_group(pending, i, used + head.bytes, budget, max_group, group_bytes, small_bytes);
+            a.small = !a.pick.empty();
+            return a;
+        }
+    return a;
 }
 
 // Whether the scheduler thread has work: a finished group to retire, shutdown
-// with nothing in flight, or a head of the queue that can be admitted now (a
-// free slot and room in the budget).  A head that does not fit in the budget
-// is not work: the scheduler sleeps until a retire frees memory (were it to
-// count, the thread would spin holding the lock that the completion callback
-// needs to report the retire).
-inline bool scheduler_has_work(bool finished, bool stop, int32_t inflight, bool pending, int64_t head_bytes,
-                               int64_t used, int64_t budget, bool free_slot)
+// with nothing in flight, or a group that pick_admission would admit now
+// (`admissible`).  Requests that cannot be admitted are not work: the
+// scheduler sleeps until a retire frees a slot or memory (were they to count,
+// the thread would spin holding the lock that the completion callback needs to
+// report the retire).
+inline bool scheduler_has_work(bool finished, bool stop, int32_t inflight, bool admissible)
 {
-    if (finished || (stop && inflight == 0))
-        return true;
-    if (!pending || used + head_bytes > budget)
-        return false;
-    return free_slot;
+    return finished || (stop && inflight == 0) || admissible;
+}
+
+// Free slots for pick_admission: any free slot, and a free slot a large group
+// may take (large groups in flight fewer than slots - small_slots).
+template <typename Srv>
+void free_slots(const Srv *S, bool &slot_free, bool &large_slot_free)
+{
+    int32_t busy = 0, large = 0;
+    for (const auto &sl : S->slots)
+        if (sl.busy) {
+            busy++;
+            large += sl.busy->small ? 0 : 1;
+        }
+    const int32_t n = (int32_t)S->slots.size();
+    const int32_t reserved = S->small_bytes > 0 ? std::min(S->small_slots, n - 1) : 0;
+    slot_free = busy < n;
+    large_slot_free = slot_free && large < n - reserved;
+}
+
+template <typename Srv>
+Admission next_admission(const Srv *S)
+{
+    bool slot_free = false, large_slot_free = false;
+    free_slots(S, slot_free, large_slot_free);
+    return pick_admission(S->pending, S->used, S->budget, S->max_group, S->group_bytes, S->small_bytes, slot_free,
+                          large_slot_free);
 }
 
 // Reports a group's device work as complete: called once per launched group,
@@ -115,12 +195,8 @@ void run_scheduler(Srv *S)
     std::unique_lock<std::mutex> lk(S->mu);
     while (true) {
         S->cv_sched.wait(lk, [&] {
-            bool free_slot = false;
-            for (const auto &sl : S->slots)
-                free_slot = free_slot || !sl.busy;
-            return scheduler_has_work(!S->finished.empty(), S->stop, S->inflight, !S->pending.empty(),
-                                      S->pending.empty() ? 0 : S->pending.front()->bytes, S->used, S->budget,
-                                      free_slot);
+            return scheduler_has_work(!S->finished.empty(), S->stop, S->inflight,
+                                      !S->finished.empty() || !next_admission(S).pick.empty());
         });
         // retire (the timings are read without the lock; a finished group's
         // slot stays busy until it is retired, so its timing state is not
@@ -160,19 +236,19 @@ void run_scheduler(Srv *S)
             break;
         // admit
         while (!S->pending.empty()) {
+            const Admission adm = next_admission(S);
+            if (adm.pick.empty())
+                break;  // no slot for the classes waiting, or no memory
+            const std::vector<size_t> &pick = adm.pick;
             int slot = -1;
             for (size_t i = 0; i < S->slots.size(); i++)
                 if (!S->slots[i].busy) {
                     slot = (int)i;
                     break;
                 }
-            if (slot < 0)
-                break;
-            const std::vector<size_t> pick = pick_group(S->pending, S->used, S->budget, S->max_group, S->group_bytes);
-            if (pick.empty())
-                break;  // the head waits for memory
             Group *G = new Group();
             G->slot = slot;
+            G->small = adm.small;
             for (size_t i : pick) {
                 auto *r = S->pending[i];
                 G->reqs.push_back(r);

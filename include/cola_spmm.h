@@ -468,7 +468,14 @@ typedef struct cola_server_opts {
     int32_t group_mib;      /* host<->device MiB (X in + Y out) past which a group takes no more
                                requests, so large requests pipeline copies against other groups'
                                launches instead of waiting for one long copy phase; 0 = 32 */
-    int32_t reserved[3];
+    int32_t small_mib;      /* size classes: a request with at most this many MiB of host<->device
+                               copies is small; one slot is kept for small requests, and a small
+                               request may be admitted ahead of a large one that waits for a slot
+                               or memory (the memory the waiting one needs stays reserved for it).
+                               0 = 16; -1 = no size classes (plain FIFO) */
+    int32_t copy_chunk_mib; /* copies move in pieces of at most this many MiB, so that another
+                               slot's copies can run between the pieces of a long one; 0 = 32 */
+    int32_t reserved[1];
 } cola_server_opts;
 
 /* Create a server on the current device (opts may be NULL).  A scheduler

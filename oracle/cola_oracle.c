@@ -673,3 +673,144 @@ int32_t orc_max_threads(void)
     return 1;
 #endif
 }
+
+/* ---------------------------------------------------------------------------
+ * Seeded R-MAT graph: the synthetic stand-in for the reference's dataset, as
+ * the library's cola_rmat_generate defines it (the reference ships no
+ * generator; its dataset is a file).  Edge e draws `scale` quadrant choices
+ * from its own splitmix64 stream (seed * 0xD1B54A32D192ED03 + e * golden
+ * ratio), 32 bits per level; self-loops are dropped, every edge is stored
+ * both ways, optional self-loops are added for every vertex, and the list is
+ * sorted by (row, col) with duplicates removed.  Values: 0 -> 1.0,
+ * 1 -> 1/deg(row), 2 -> 1/sqrt(deg(row) deg(col)).  Two-call protocol: row ==
+ * NULL returns the entry count in *nnz.  The bench's reference leg uses this
+ * restatement so that it loads nothing of the product.
+ * ------------------------------------------------------------------------- */
+static uint64_t orc_splitmix64(uint64_t *s)
+{
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* LSD radix sort of keys only (16-bit digits over key_bits). */
+static int radix_sort_keys(uint64_t *key, int64_t n, int key_bits)
+{
+    if (n <= 1)
+        return ORC_OK;
+    uint64_t *tmp = (uint64_t *)malloc((size_t)n * sizeof(uint64_t));
+    int64_t *cnt = (int64_t *)malloc(65536 * sizeof(int64_t));
+    if (!tmp || !cnt) {
+        free(tmp);
+        free(cnt);
+        return ORC_ERR;
+    }
+    uint64_t *src = key, *dst = tmp;
+    for (int shift = 0; shift < key_bits; shift += 16) {
+        memset(cnt, 0, 65536 * sizeof(int64_t));
+        for (int64_t i = 0; i < n; i++)
+            cnt[(src[i] >> shift) & 0xFFFF]++;
+        int64_t s = 0;
+        for (int d = 0; d < 65536; d++) {
+            int64_t c = cnt[d];
+            cnt[d] = s;
+            s += c;
+        }
+        for (int64_t i = 0; i < n; i++)
+            dst[cnt[(src[i] >> shift) & 0xFFFF]++] = src[i];
+        uint64_t *t = src;
+        src = dst;
+        dst = t;
+    }
+    if (src != key)
+        memcpy(key, src, (size_t)n * sizeof(uint64_t));
+    free(tmp);
+    free(cnt);
+    return ORC_OK;
+}
+
+int orc_rmat_generate(int32_t scale, double deg, double a, double b, double c, uint64_t seed,
+                      int32_t self_loops, int32_t value_kind, int32_t *row, int32_t *col, float *val,
+                      int64_t capacity, int64_t *nnz)
+{
+    if (scale < 1 || scale > 30 || !(deg > 0) || a < 0 || b < 0 || c < 0 || a + b + c > 1.0 || !nnz)
+        return ORC_ERR;
+    const int64_t n = (int64_t)1 << scale;
+    const int64_t m = (int64_t)ceil(deg * (double)n / 2.0);
+    const int64_t cap = 2 * m + (self_loops ? n : 0);
+    uint64_t *keys = (uint64_t *)malloc((size_t)cap * sizeof(uint64_t));
+    unsigned char *keep = (unsigned char *)malloc((size_t)m);
+    if (!keys || !keep) {
+        free(keys);
+        free(keep);
+        return ORC_ERR;
+    }
+    const double ab = a + b, abc = a + b + c;
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < m; e++) {
+        uint64_t st = seed * 0xD1B54A32D192ED03ull + (uint64_t)e * 0x9E3779B97F4A7C15ull;
+        uint64_t u = 0, v = 0, bits = 0;
+        for (int l = 0; l < scale; l++) {
+            if ((l & 1) == 0)
+                bits = orc_splitmix64(&st);
+            const double p = (double)((bits >> ((l & 1) * 32)) & 0xFFFFFFFFull) * (1.0 / 4294967296.0);
+            const uint64_t rb = p >= ab ? 1 : 0;
+            const uint64_t cb = ((p >= a && p < ab) || p >= abc) ? 1 : 0;
+            u = (u << 1) | rb;
+            v = (v << 1) | cb;
+        }
+        keep[e] = u != v;
+        keys[2 * e] = (u << scale) | v;
+        keys[2 * e + 1] = (v << scale) | u;
+    }
+    int64_t k = 0;
+    for (int64_t e = 0; e < m; e++)
+        if (keep[e]) {
+            keys[k++] = keys[2 * e];
+            keys[k++] = keys[2 * e + 1];
+        }
+    free(keep);
+    if (self_loops)
+        for (int64_t i = 0; i < n; i++)
+            keys[k++] = ((uint64_t)i << scale) | (uint64_t)i;
+    if (radix_sort_keys(keys, k, 2 * scale) != ORC_OK) {
+        free(keys);
+        return ORC_ERR;
+    }
+    int64_t u = 0;
+    for (int64_t i = 0; i < k; i++)
+        if (i == 0 || keys[i] != keys[i - 1])
+            keys[u++] = keys[i];
+    *nnz = u;
+    if (!row) {
+        free(keys);
+        return ORC_OK;
+    }
+    if (u > capacity || !col || !val) {
+        free(keys);
+        return ORC_ERR;
+    }
+    int32_t *dg = (int32_t *)calloc((size_t)n, sizeof(int32_t));
+    if (!dg) {
+        free(keys);
+        return ORC_ERR;
+    }
+    const uint64_t mask = ((uint64_t)1 << scale) - 1;
+    for (int64_t i = 0; i < u; i++) {
+        row[i] = (int32_t)(keys[i] >> scale);
+        col[i] = (int32_t)(keys[i] & mask);
+        dg[row[i]]++;
+    }
+    for (int64_t i = 0; i < u; i++) {
+        if (value_kind == 1)
+            val[i] = (float)(1.0 / (double)dg[row[i]]);
+        else if (value_kind == 2)
+            val[i] = (float)(1.0 / sqrt((double)dg[row[i]] * (double)dg[col[i]]));
+        else
+            val[i] = 1.0f;
+    }
+    free(dg);
+    free(keys);
+    return ORC_OK;
+}

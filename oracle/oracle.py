@@ -46,6 +46,8 @@ def lib():
         L.orc_spmm_partition_f64.argtypes = [I32, I32, P, P, P, P, I64, P, P, P, P, I64, P, I64, I32, P, I64]
         L.orc_spmm_partitions_f32_omp.argtypes = [I32, I32] + [P] * 15 + [I64, I32, P, I64, I32]
         L.orc_max_threads.restype = I32
+        L.orc_rmat_generate.argtypes = [I32, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_uint64, I32, I32, P, P, P, I64, P]
         _lib = L
     return _lib
 
@@ -132,6 +134,25 @@ def global_csr(num_nodes, row, col, val=None):
                         ctypes.byref(m)) != 0:
         raise RuntimeError("orc_global_csr failed")
     return rp, ci[: m.value], vo[: m.value]
+
+
+def rmat(scale, avg_degree, seed, a=0.57, b=0.19, c=0.19, self_loops=False, values=2):
+    """The seeded R-MAT graph the library's cola_rmat_generate defines,
+    restated in C (orc_rmat_generate).  values: 0 ones, 1 1/deg(row),
+    2 D^-1/2 A D^-1/2.  Returns (num_nodes, row, col, val)."""
+    L = lib()
+    cnt = ctypes.c_int64()
+    args = (int(scale), float(avg_degree), float(a), float(b), float(c), ctypes.c_uint64(int(seed)),
+            1 if self_loops else 0, int(values))
+    if L.orc_rmat_generate(*args, None, None, None, 0, ctypes.byref(cnt)) != 0:
+        raise RuntimeError("orc_rmat_generate failed")
+    m = cnt.value
+    row = np.zeros(max(m, 1), np.int32)
+    col = np.zeros(max(m, 1), np.int32)
+    val = np.zeros(max(m, 1), np.float32)
+    if L.orc_rmat_generate(*args, _ptr(row), _ptr(col), _ptr(val), m, ctypes.byref(cnt)) != 0:
+        raise RuntimeError("orc_rmat_generate failed")
+    return 1 << int(scale), row[:m], col[:m], val[:m]
 
 
 def workgroup_cols(num_nodes, row, col, nparts, gs, stage):

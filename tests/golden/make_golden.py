@@ -16,7 +16,8 @@ writes, so the parity tests can run where the reference tree is absent:
 
 Usage (in a container that has the reference tree and oracle/_ref built)::
 
-    python tests/golden/make_golden.py [--ref-root /root/reference]
+    python tests/golden/make_golden.py [--ref-root DIR]   (default: $COLA_REF_ROOT, else
+    a checkout named `reference` beside this repository's directory)
 
 The inputs are generated here from fixed seeds (numpy PCG64) and stored in the
 fixture next to the outputs.
@@ -104,7 +105,9 @@ def ref_nnz_split(lib, rowIdx, rowPtr, nnz):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    repo = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    ap.add_argument("--ref-root", default=os.environ.get("COLA_REF_ROOT") or
+                    os.path.join(os.path.dirname(repo), "reference"))
     args = ap.parse_args()
     par = load_module(os.path.join(args.ref_root, "prep_torch_par.py"), "ref_prep_torch_par")
     ppl = load_module(os.path.join(args.ref_root, "prep_torch_ppl.py"), "ref_prep_torch_ppl")

@@ -8,7 +8,11 @@
 //
 // Scenarios: budget (the budget admits one request at a time, requests
 // submitted while others run), mix (large budget, mixed keys, bursts), fail
-// (some launches fail), stop (shutdown with work queued).  Every wait has a
+// (some launches fail), stop (shutdown with work queued), sizes / sizes_fifo
+// (four requests with 20 ms of copies each arrive first, then a small request
+// every millisecond; the fake device serves its queue round robin in 0.5 ms
+// turns, as the copy engine takes the pieces of chunked copies; with size
+// classes on, and off).  Every wait has a
 // deadline; a missed deadline prints STALL and exits 1 (a scheduler that spins
 // holding its lock stalls the program instead: the caller's timeout catches
 // that).  Prints one "ok ..." line with the counters on success.
@@ -58,6 +62,8 @@ struct FakeServer {
     int64_t budget = 0, used = 0, peak_used = 0;
     int32_t max_group = 16;
     int64_t group_bytes = 32 << 20;
+    int64_t small_bytes = 0;  // size classes off unless a scenario sets them
+    int32_t small_slots = 1;
     bool stop = false;
     int32_t inflight = 0, max_inflight = 0, groups_launched = 0, max_group_seen = 0;
     int64_t completed = 0, failed = 0;
@@ -70,6 +76,8 @@ struct FakeServer {
     std::condition_variable dev_cv;
     std::deque<std::pair<Group *, int>> dev_queue;  // group, microseconds of "work"
     bool dev_stop = false;
+    int chunk_us = 1 << 30;     // the device serves queued groups round robin, this long a turn
+    int us_per_copy_byte = 0;   // > 0: a group's work is its copy bytes times this (the host link)
     int fail_every = 0;  // > 0: launches whose head id % fail_every == 1 fail
     std::mt19937_64 rng{1};
 };
@@ -80,7 +88,14 @@ struct FakeDevice {
         if (S->fail_every > 0 && G->reqs.front()->id % (uint64_t)S->fail_every == 1)
             return 2;  // as a CUDA error would
         std::lock_guard<std::mutex> lk(S->dev_mu);
-        S->dev_queue.emplace_back(G, (int)(S->rng() % 400));
+        int us = (int)(S->rng() % 400);
+        if (S->us_per_copy_byte > 0) {
+            int64_t copy = 0;
+            for (const Req *r : G->reqs)
+                copy += r->copy_bytes;
+            us = (int)(copy * S->us_per_copy_byte);
+        }
+        S->dev_queue.emplace_back(G, us);
         S->dev_cv.notify_all();
         return 0;
     }
@@ -102,8 +117,14 @@ void device_thread(FakeServer *S)
             return;
         auto job = S->dev_queue.front();
         S->dev_queue.pop_front();
+        const int turn = std::min(job.second, S->chunk_us);
         lk.unlock();
-        std::this_thread::sleep_for(std::chrono::microseconds(job.second));
+        std::this_thread::sleep_for(std::chrono::microseconds(turn));
+        if (turn < job.second) {  // the rest of this group's work waits for its next turn
+            lk.lock();
+            S->dev_queue.emplace_back(job.first, job.second - turn);
+            continue;
+        }
         cola::group_finished(S, job.first, now_s());  // no lock of the server held here
         lk.lock();
     }
@@ -128,12 +149,19 @@ int main(int argc, char **argv)
     S.rng.seed(seed);
     std::mt19937_64 rng(seed * 7 + 1);
     const bool budget_case = !std::strcmp(scen, "budget");
-    const int nreq = !std::strcmp(scen, "stop") ? 300 : 400;
+    const bool sizes_case = !std::strncmp(scen, "sizes", 5);
+    const int nlarge = 4;
+    const int nreq = !std::strcmp(scen, "stop") ? 300 : (sizes_case ? nlarge + 60 : 400);
     S.slots.resize(4);
     S.max_group = 8;
     S.group_bytes = 3000;
     S.budget = budget_case ? 1500 : 1000000;  // budget: one request (1000 bytes) at a time
     S.fail_every = !std::strcmp(scen, "fail") ? 5 : 0;
+    if (sizes_case) {
+        S.us_per_copy_byte = 1;
+        S.chunk_us = 500;
+        S.small_bytes = !std::strcmp(scen, "sizes") ? 100 : 0;
+    }
     std::thread dev(device_thread, &S);
     std::thread sched([&] { cola::run_scheduler<FakeServer, FakeDevice>(&S); });
 
@@ -145,6 +173,12 @@ int main(int argc, char **argv)
         r->xdt = budget_case ? 0 : (int)(rng() % 2);
         r->bytes = budget_case ? 1000 : 100 + (int64_t)(rng() % 900);
         r->copy_bytes = 50 + (int64_t)(rng() % 1000);
+        if (sizes_case) {
+            r->K = 64;
+            r->xdt = 0;
+            r->bytes = 1000;
+            r->copy_bytes = i < nlarge ? 20000 : 20;  // 20 ms and 20 us of copies
+        }
         {
             std::lock_guard<std::mutex> lk(S.mu);
             r->t_submit = now_s();
@@ -152,8 +186,12 @@ int main(int argc, char **argv)
         }
         S.cv_sched.notify_all();
         reqs.push_back(r);
-        if (rng() % 4 == 0)  // bursts, with requests arriving while others run
+        if (sizes_case) {
+            if (i >= nlarge - 1)
+                std::this_thread::sleep_for(std::chrono::milliseconds(1));
+        } else if (rng() % 4 == 0) {  // bursts, with requests arriving while others run
             std::this_thread::sleep_for(std::chrono::microseconds(rng() % 300));
+        }
     }
     const auto deadline = std::chrono::steady_clock::now() + std::chrono::seconds(30);
     if (!std::strcmp(scen, "stop")) {
@@ -217,11 +255,21 @@ int main(int argc, char **argv)
         else
             other++;
     }
+    // latency (submission to completion) of the small and the large requests, in microseconds
+    int64_t small_max = 0, large_min = -1;
+    for (size_t i = 0; i < reqs.size(); i++) {
+        const int64_t us = (int64_t)((reqs[i]->t_done - reqs[i]->t_submit) * 1e6);
+        if (sizes_case && (int)i >= nlarge)
+            small_max = std::max(small_max, us);
+        else if (sizes_case)
+            large_min = large_min < 0 ? us : std::min(large_min, us);
+    }
     std::printf("ok done=%lld failed=%lld cancelled=%lld other=%lld used=%lld peak=%lld budget=%lld "
-                "max_inflight=%d max_group=%d groups=%d completed=%lld sfailed=%lld\n",
+                "max_inflight=%d max_group=%d groups=%d completed=%lld sfailed=%lld small_max_us=%lld "
+                "large_min_us=%lld\n",
                 (long long)done, (long long)failed, (long long)cancelled, (long long)other, (long long)S.used,
                 (long long)S.peak_used, (long long)S.budget, S.max_inflight, S.max_group_seen, S.groups_launched,
-                (long long)S.completed, (long long)S.failed);
+                (long long)S.completed, (long long)S.failed, (long long)small_max, (long long)large_min);
     for (Req *r : reqs)
         delete r;
     return 0;

@@ -112,23 +112,90 @@ def test_policy_edge_cases(policy_exe):
 def test_scheduler_wake_condition(policy_exe):
     import itertools
     rows, want = [], []
-    for finished, stop, inflight, pending, fits, free_slot in itertools.product([0, 1], [0, 1], [0, 2], [0, 1],
-                                                                              [0, 1], [0, 1]):
-        used, budget = 500, 1000
-        head = 400 if fits else 600
-        rows.append("{} {} {} {} {} {} {} {}".format(finished, stop, inflight, pending, head if pending else 0, used,
-                                                     budget, free_slot))
-        want.append(int(bool(finished) or (bool(stop) and inflight == 0) or
-                        (bool(pending) and bool(fits) and bool(free_slot))))
+    for finished, stop, inflight, admissible in itertools.product([0, 1], [0, 1], [0, 2], [0, 1]):
+        rows.append("{} {} {} {}".format(finished, stop, inflight, admissible))
+        want.append(int(bool(finished) or (bool(stop) and inflight == 0) or bool(admissible)))
     res = subprocess.run([policy_exe, "wake"], input="{}\n{}\n".format(len(rows), "\n".join(rows)),
                          capture_output=True, text=True, check=True)
     got = [int(v) for v in res.stdout.split()]
     assert got == want
     # the stall this rules out: requests queued behind a head that waits for
-    # memory, a slot free, nothing finished yet -> the scheduler must sleep
-    res = subprocess.run([policy_exe, "wake"], input="1\n0 0 1 1 600 500 1000 1\n", capture_output=True, text=True,
+    # memory, a slot free, nothing finished yet -> nothing is admissible, so
+    # the scheduler must sleep
+    assert admit(policy_exe, [(500, 1000, 8, 10 ** 6, 0, 1, 1, [(64, 0, 0, 600, 1), (64, 0, 0, 100, 1)])]) == \
+        [("L", [])]
+
+
+def admit(exe, cases):
+    lines = [str(len(cases))]
+    for used, budget, max_group, group_bytes, small, slot_free, large_free, reqs in cases:
+        lines.append("{} {} {} {} {} {} {} {}".format(used, budget, max_group, group_bytes, small, slot_free,
+                                                        large_free, len(reqs)))
+        lines += ["{} {} {} {} {}".format(*r) for r in reqs]
+    res = subprocess.run([exe, "admit"], input="\n".join(lines) + "\n", capture_output=True, text=True,
                          check=True)
-    assert res.stdout.split() == ["0"]
+    out = []
+    for line in res.stdout.splitlines():
+        f = line.split()
+        out.append((f[0], [] if f[1:] == ["-"] else [int(v) for v in f[1:]]))
+    assert len(out) == len(cases)
+    return out
+
+
+def test_size_classes_admission(policy_exe):
+    """pick_admission: a small request (copies at most small_bytes) passes a
+    large head that waits for a slot, in the memory left beside the head's; a
+    head that waits for memory is passed by nothing; a group holds one size
+    class; with the classes off it is pick_group."""
+    L = (64, 0, 0, 100, 10 ** 6)     # large: 1 MB of copies in these units
+    Sm = (64, 0, 0, 10, 5)           # small
+    S16 = (16, 0, 0, 10, 5)          # small, another key
+    big = 10 ** 9
+    cases = [
+        (0, big, 8, 10 ** 7, 100, 1, 1, [L, Sm, Sm]),      # a large slot is free: FIFO, the large head alone
+        (0, big, 8, 10 ** 7, 100, 1, 0, [L, Sm, L, Sm]),   # no large slot: the small ones pass, only small join
+        (0, big, 8, 10 ** 7, 100, 1, 0, [L, S16, Sm, S16]),  # the first small opens; its key only
+        (0, big, 8, 10 ** 7, 100, 0, 0, [L, Sm]),          # no slot at all: nothing
+        (0, 150, 8, 10 ** 7, 100, 1, 1, [L, Sm, Sm]),      # room for the head: it goes, alone (one class)
+        (60, 150, 8, 10 ** 7, 100, 1, 0, [L, Sm, Sm, Sm]),  # the head waits for memory: nothing passes
+        (20, 140, 8, 10 ** 7, 100, 1, 0, [L, Sm, Sm, Sm]),  # 120 with the head's 100 kept: two smalls fit
+        (0, big, 8, 10 ** 7, 100, 1, 0, [Sm, L, Sm]),      # small head: a small group, the large one skipped
+        (0, big, 8, 10 ** 7, 0, 1, 0, [L, Sm, Sm]),        # classes off: plain FIFO whatever the slots
+        (0, big, 2, 10 ** 7, 100, 1, 0, [L, Sm, Sm, Sm]),  # max_group caps the small group
+    ]
+    got = admit(policy_exe, cases)
+    assert got == [("L", [0]), ("S", [1, 3]), ("S", [1, 3]), ("L", []), ("L", [0]), ("L", []), ("S", [1, 2]),
+                   ("S", [0, 2]), ("L", [0, 1, 2]), ("S", [1, 2])]
+
+
+def test_size_classes_random_queues_never_starve_the_head(policy_exe):
+    """On random queues: whatever pick_admission admits fits the budget and
+    holds one size class; a head that waits for memory is passed by nothing;
+    a small group passing a large head leaves the head's bytes free; with a
+    slot its class may take and room for it, the head is admitted first."""
+    rng = np.random.Generator(np.random.Philox(21))
+    cases = []
+    for _ in range(2000):
+        n = int(rng.integers(1, 20))
+        reqs = [(64, 0, 0, int(rng.integers(1, 500)), int(rng.choice([5, 50, 5000]))) for _ in range(n)]
+        used = int(rng.integers(0, 1000))
+        cases.append((used, used + int(rng.integers(0, 2000)), int(rng.integers(1, 9)), 10 ** 6, 100,
+                      int(rng.integers(0, 2)), int(rng.integers(0, 2)), reqs))
+    for case, (cls, pick) in zip(cases, admit(policy_exe, cases)):
+        used, budget, max_group, _, small, slot_free, large_free, reqs = case
+        head = reqs[0]
+        if not slot_free:
+            assert pick == []
+            continue
+        assert used + sum(reqs[i][3] for i in pick) <= budget and len(pick) <= max_group
+        assert len({reqs[i][4] <= small for i in pick}) <= 1
+        if used + head[3] > budget:
+            assert pick == []
+        elif head[4] <= small or large_free:
+            assert pick and pick[0] == 0 and cls == ("S" if head[4] <= small else "L")
+        elif pick:
+            assert cls == "S" and pick[0] > 0 and all(reqs[i][4] <= small for i in pick)
+            assert used + head[3] + sum(reqs[i][3] for i in pick) <= budget
 
 
 @pytest.fixture(scope="module")
@@ -190,3 +257,18 @@ def test_scheduler_loop_has_no_data_race(tmp_path):
         res = subprocess.run([exe, scenario, "9"], capture_output=True, text=True, timeout=300)
         assert "ThreadSanitizer" not in res.stderr, res.stderr[:4000]
         assert res.returncode == 0 and res.stdout.startswith("ok "), res.stdout + res.stderr[:2000]
+
+
+def test_small_requests_are_not_held_behind_large_copies(sched_exe):
+    """Four requests with 20 ms of copies each arrive first, then a small
+    request every millisecond, on a fake device that serves its queue round
+    robin in 0.5 ms turns (chunked copies).  Plain FIFO: the large requests
+    take every slot and each small one waits for one of them to finish.  With
+    size classes one slot stays free for small requests, which finish within a
+    few turns while the large copies are still running."""
+    on = run_sched(sched_exe, "sizes", 3)
+    off = run_sched(sched_exe, "sizes_fifo", 3)
+    for c in (on, off):
+        assert c["done"] == 64 and c["other"] == 0 and c["used"] == 0
+    assert on["small_max_us"] < 10000 < on["large_min_us"]
+    assert off["small_max_us"] > 15000
