@@ -122,6 +122,10 @@ SIGNATURES = {
     "cola_ppl0_batch_buffer_spmm": (I32, [P, P, P] + [P] * 8 + [I32] * 7 + [P]),
     "cola_ppl0_batch_buffer_spmm_noalloc": (I32, [P, P] + [P] * 8 + [I32] * 7 + [P]),
     "cola_ppl_batch_spmm": (I32, [P, P, P, P, P, P] + [I32] * 5 + [P] + [I32] * 5 + [P]),
+    "cola_zip_rows_create": (I32, [P] * 8 + [I32] * 6 + [P, P]),
+    "cola_zip_rows_spmm": (I32, [P, P, P, I32, P]),
+    "cola_zip_rows_free": (I32, [P]),
+    "cola_zip_rows_get_info": (I32, [P, P, P, P, P]),
     "cola_batching_data_ppl": (I32, [P, P, P, I32, I32, I32, I32, P]),
     "cola_graph_upload": (I32, [P, P, P, P]),
     "cola_graph_free": (I32, [P]),

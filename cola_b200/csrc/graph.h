@@ -91,6 +91,12 @@ struct cola_graph {
 
 namespace cola {
 void graph_release(cola_graph *g);
+// The row-view graph of an nrows x ncols COO in device memory (entries sorted
+// by (row, col), duplicates merged, hub segments and row-block tasks), for
+// the row-major schedule; ncols >= nrows.
+cola_status graph_build_device_rect(int32_t nrows, int32_t ncols, int64_t nnz, const int32_t *row, const int32_t *col,
+                                    const float *val, const cola_upload_opts *opts, cudaStream_t st, cola_graph *&out,
+                                    const char *who);
 cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *opts, cola_graph *&out,
                          cudaStream_t st);
 }  // namespace cola

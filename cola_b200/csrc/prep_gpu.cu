@@ -163,12 +163,12 @@ struct ChunksF {
 // partitioning kernels
 // ---------------------------------------------------------------------------
 
-__global__ void check_coo_kernel(const int32_t *row, const int32_t *col, int64_t n, int32_t N,
+__global__ void check_coo_kernel(const int32_t *row, const int32_t *col, int64_t n, int32_t NR, int32_t NC,
                                  unsigned long long *first_bad)
 {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t r = row[i], c = col[i];
-        if (r < 0 || r >= N || c < 0 || c >= N)
+        if (r < 0 || r >= NR || c < 0 || c >= NC)
             atomicMin(first_bad, (unsigned long long)i);
     }
 }
@@ -709,13 +709,16 @@ static cola_status exclusive_scan(F f, int64_t n, uint32_t *out, uint32_t *d_tot
     return COLA_SUCCESS;
 }
 
+// Every entry inside NR rows x NC columns (NC < 0: NC = NR).
 static cola_status check_range(const int32_t *row, const int32_t *col, int64_t n, int32_t N, Scratch &sc,
-                               const char *who)
+                               const char *who, int32_t NC = -1)
 {
+    if (NC < 0)
+        NC = N;
     unsigned long long *bad = nullptr, h_bad = 0;
     COLA_TRY(sc.get(bad, 1));
     COLA_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(*bad), sc.st));
-    check_coo_kernel<<<grid_stride_blocks(n), 256, 0, sc.st>>>(row, col, n, N, bad);
+    check_coo_kernel<<<grid_stride_blocks(n), 256, 0, sc.st>>>(row, col, n, N, NC, bad);
     t_launches++;
     COLA_CUDA(cudaGetLastError());
     COLA_CUDA(cudaMemcpyAsync(&h_bad, bad, sizeof(h_bad), cudaMemcpyDeviceToHost, sc.st));
@@ -724,7 +727,7 @@ static cola_status check_range(const int32_t *row, const int32_t *col, int64_t n
         int32_t r = 0, c = 0;
         cudaMemcpy(&r, row + h_bad, 4, cudaMemcpyDeviceToHost);
         cudaMemcpy(&c, col + h_bad, 4, cudaMemcpyDeviceToHost);
-        return fail(COLA_ERROR_INVALID_ARGUMENT, "%s: entry %llu (%d, %d) outside %d x %d", who, h_bad, r, c, N, N);
+        return fail(COLA_ERROR_INVALID_ARGUMENT, "%s: entry %llu (%d, %d) outside %d x %d", who, h_bad, r, c, N, NC);
     }
     return COLA_SUCCESS;
 }
@@ -886,11 +889,15 @@ static cola_status partition_build_device(int32_t N, int64_t nnz, const int32_t 
 // host: entries sorted by (row, col) with duplicates merged (values summed in
 // input order), row pointers, hub segments and row-block tasks.  The result is
 // identical to the upload of the same COO's partitions, array for array.
+// NC > 0: a rectangular N x NC matrix (rows N, columns NC >= N), as one
+// partition's rows over the global columns are.
 static cola_status graph_build_device(int32_t N, int64_t nnz, const int32_t *row, const int32_t *col,
                                       const float *val, int32_t nparts, const cola_upload_opts *opts, cudaStream_t st,
-                                      cola_graph *&out)
+                                      cola_graph *&out, int32_t NC = -1, const char *who = "cola_graph_build_device")
 {
-    const char *who = "cola_graph_build_device";
+    if (NC < 0)
+        NC = N;
+    COLA_REQUIRE(NC >= N, COLA_ERROR_INVALID_ARGUMENT, "%s: %d columns < %d rows", who, NC, N);
     COLA_REQUIRE(N >= 0 && nnz >= 0 && nparts >= 1, COLA_ERROR_INVALID_ARGUMENT, "%s: N=%d nnz=%lld nparts=%d", who,
                  N, (long long)nnz, nparts);
     COLA_REQUIRE(nnz == 0 || (row && col), COLA_ERROR_INVALID_ARGUMENT, "%s: null COO arrays", who);
@@ -903,7 +910,7 @@ static cola_status graph_build_device(int32_t N, int64_t nnz, const int32_t *row
     const int64_t seg = opts && opts->hub_segment > 0 ? opts->hub_segment : 256;
     const int64_t te = opts && opts->task_entries > 0 ? opts->task_entries : 128;
     const int64_t npp = ((int64_t)N + nparts - 1) / nparts;
-    const int cb = bits_for(N > 0 ? (uint64_t)N - 1 : 0);
+    const int cb = bits_for(NC > 0 ? (uint64_t)NC - 1 : 0);  // column bits; rows (< N <= NC) fit in as many
 
     std::unique_ptr<cola_graph, void (*)(cola_graph *)> g(new (std::nothrow) cola_graph(), graph_release);
     COLA_REQUIRE(g, COLA_ERROR_OUT_OF_MEMORY, "%s: host allocation failed", who);
@@ -933,7 +940,7 @@ static cola_status graph_build_device(int32_t N, int64_t nnz, const int32_t *row
         COLA_TRY(sc.reserve(bytes));
     }
     if (nnz > 0)
-        COLA_TRY(check_range(row, col, nnz, N, sc, who));
+        COLA_TRY(check_range(row, col, nnz, N, sc, who, NC));
     uint32_t *d_total = nullptr;
     COLA_TRY(sc.get(d_total, 1));
     uint64_t *ukey = nullptr;
@@ -1061,6 +1068,14 @@ static cola_status graph_build_device(int32_t N, int64_t nnz, const int32_t *row
 }
 
 }  // namespace pg
+
+cola_status graph_build_device_rect(int32_t nrows, int32_t ncols, int64_t nnz, const int32_t *row, const int32_t *col,
+                                    const float *val, const cola_upload_opts *opts, cudaStream_t st, cola_graph *&out,
+                                    const char *who)
+{
+    return pg::graph_build_device(nrows, nnz, row, col, val, 1, opts, st, out, ncols, who);
+}
+
 }  // namespace cola
 
 using namespace cola;

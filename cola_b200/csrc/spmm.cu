@@ -10,6 +10,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include <cuda.h>  // CUcontext and CUresult, for the context id read through the runtime
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -1344,21 +1345,54 @@ static __device__ __align__(256) float g_noalloc_stage[COLA_NOALLOC_STAGE_FLOATS
 
 namespace cola {
 
+// Unique id of the calling thread's current CUDA context (cuCtxGetId, reached
+// through the runtime's driver entry points, so the library does not link the
+// driver library itself); 0 if it cannot be read.
+static unsigned long long current_context_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
 // Device address of g_noalloc_stage on the current device.  In host code the
 // array's name only stands in for the symbol, so the address is looked up with
-// cudaGetSymbolAddress, once per device (the first call on each device).
+// cudaGetSymbolAddress on the first call on each device, and again whenever
+// that device's context is no longer the one the address was taken in (after
+// cudaDeviceReset the array lives in a new context, at a new address).
 static cola_status noalloc_stage(float **out)
 {
     static std::mutex mu;
     static float *addr[64] = {nullptr};
+    static unsigned long long ctx_of[64] = {0};
     int dev = 0;
     COLA_CUDA(cudaGetDevice(&dev));
     COLA_REQUIRE(dev >= 0 && dev < 64, COLA_ERROR_UNSUPPORTED, "noalloc staging: device %d out of range", dev);
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lk(mu);
-    if (!addr[dev]) {
+    if (!addr[dev] || ctx == 0 || ctx != ctx_of[dev]) {
         void *p = nullptr;
-        COLA_CUDA(cudaGetSymbolAddress(&p, g_noalloc_stage));
+        COLA_CUDA(cudaGetSymbolAddress(&p, g_noalloc_stage));  // also makes the device's context current
         addr[dev] = static_cast<float *>(p);
+        ctx_of[dev] = current_context_id();
     }
     *out = addr[dev];
     return COLA_SUCCESS;

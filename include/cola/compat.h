@@ -17,6 +17,15 @@
  *  - the multi-stage schedule (group_size < nranks) runs all PEs together:
  *    distSpMM_ppl_batch_all().  The per-PE wrapper supports group_size == nranks,
  *    which is what P virtual partitions on one GPU map to.
+ *  - ppl0_batch_SpMM (and the wrapper, which calls it) on the arrays of a
+ *    d_csr_zip / d_csc_zip pair builds, on its first call for that pair and
+ *    chunk range, the pair's row view on the device (cola_zip_rows_create: it
+ *    synchronises the stream once) and keeps it until either holder is
+ *    destroyed; every call then runs the row-major schedule on it (one writer
+ *    per row, no atomics, the same bits every call) instead of the chunk
+ *    kernel.  The result is the same product; arrays not owned by a holder
+ *    run the chunk kernel.  cola_compat::set_row_view_cache(false) turns the
+ *    cache off.
  */
 #ifndef COLA_COMPAT_H
 #define COLA_COMPAT_H
@@ -26,8 +35,11 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -60,6 +72,90 @@ inline T *upload(const std::vector<T> &v, const char *where)
     if (!v.empty())
         check_cuda(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), where);
     return p;
+}
+
+// Row views of d_csr_zip / d_csc_zip pairs, built on first use by
+// ppl0_batch_SpMM and dropped when either holder is destroyed.  Holders enter
+// the registry with their device arrays, so arrays a holder does not own are
+// never looked up in it.
+struct zip_registry {
+    using arrays = std::tuple<const void *, const void *, const void *, const void *>;
+    using view_key = std::tuple<const void *, const void *, int, int, int, int, int, int>;
+    std::mutex mu;
+    std::map<const void *, arrays> csr, csc;  // holder -> its four device arrays
+    std::map<view_key, cola_zip_rows *> views;
+    bool enabled = true;
+};
+
+inline zip_registry &registry()
+{
+    static zip_registry r;
+    return r;
+}
+
+inline void set_row_view_cache(bool on)
+{
+    std::lock_guard<std::mutex> lk(registry().mu);
+    registry().enabled = on;
+}
+
+inline void register_holder(bool is_csr, const void *holder, zip_registry::arrays a)
+{
+    std::lock_guard<std::mutex> lk(registry().mu);
+    (is_csr ? registry().csr : registry().csc)[holder] = a;
+}
+
+// Forget a holder and free the row views built on its arrays.
+inline void forget_holder(bool is_csr, const void *holder)
+{
+    zip_registry &R = registry();
+    std::lock_guard<std::mutex> lk(R.mu);
+    (is_csr ? R.csr : R.csc).erase(holder);
+    for (auto it = R.views.begin(); it != R.views.end();) {
+        if ((is_csr ? std::get<0>(it->first) : std::get<1>(it->first)) == holder) {
+            cola_zip_rows_free(it->second);
+            it = R.views.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
+// The row view for these arrays and chunk range when both blocks belong to
+// holders (built now if this is the first call), else nullptr.
+inline cola_zip_rows *cached_row_view(const int *csr_rowPtr_l, const int *csr_colIdx_l, const int *csr_rowIdx_zip_l,
+                                      const float *csr_val_l, const int *csc_colPtr_r, const int *csc_rowIdx_r,
+                                      const int *csc_colIdx_zip_r, const float *csc_val_r, int local_row_lb,
+                                      int remote_col_lb, int local_row_num, int remote_col_num, int nodesPerPE,
+                                      int peid, cudaStream_t stream)
+{
+    zip_registry &R = registry();
+    std::lock_guard<std::mutex> lk(R.mu);
+    if (!R.enabled)
+        return nullptr;
+    const zip_registry::arrays want_l{csr_rowPtr_l, csr_colIdx_l, csr_rowIdx_zip_l, csr_val_l};
+    const zip_registry::arrays want_r{csc_colPtr_r, csc_rowIdx_r, csc_colIdx_zip_r, csc_val_r};
+    const void *hl = nullptr, *hr = nullptr;
+    for (const auto &kv : R.csr)
+        if (kv.second == want_l)
+            hl = kv.first;
+    for (const auto &kv : R.csc)
+        if (kv.second == want_r)
+            hr = kv.first;
+    if (!hl || !hr)
+        return nullptr;
+    const zip_registry::view_key k{hl, hr, local_row_lb, remote_col_lb, local_row_num, remote_col_num, nodesPerPE,
+                                   peid};
+    auto it = R.views.find(k);
+    if (it != R.views.end())
+        return it->second;
+    cola_zip_rows *h = nullptr;
+    check(cola_zip_rows_create(csr_rowPtr_l, csr_colIdx_l, csr_rowIdx_zip_l, csr_val_l, csc_colPtr_r, csc_rowIdx_r,
+                               csc_colIdx_zip_r, csc_val_r, local_row_lb, remote_col_lb, local_row_num,
+                               remote_col_num, nodesPerPE, peid, (cola_stream_t)stream, &h),
+          "ppl0_batch_SpMM (row view)");
+    R.views[k] = h;
+    return h;
 }
 
 }  // namespace cola_compat
@@ -97,11 +193,13 @@ struct d_csc_zip {
         d_csc_rowIdx = cola_compat::upload(rowIdx, "d_csc_zip");
         d_csc_colIdx_zip = cola_compat::upload(colIdx_zip, "d_csc_zip");
         d_csc_val = cola_compat::upload(val, "d_csc_zip");
+        cola_compat::register_holder(false, this, {d_csc_colPtr, d_csc_rowIdx, d_csc_colIdx_zip, d_csc_val});
     }
     d_csc_zip(const d_csc_zip &) = delete;
     d_csc_zip &operator=(const d_csc_zip &) = delete;
     ~d_csc_zip()
     {
+        cola_compat::forget_holder(false, this);
         cudaFree(d_csc_colPtr);
         cudaFree(d_csc_rowIdx);
         cudaFree(d_csc_colIdx_zip);
@@ -121,11 +219,13 @@ struct d_csr_zip {
         d_csr_colIdx = cola_compat::upload(colIdx, "d_csr_zip");
         d_csr_rowIdx_zip = cola_compat::upload(rowIdx_zip, "d_csr_zip");
         d_csr_val = cola_compat::upload(val, "d_csr_zip");
+        cola_compat::register_holder(true, this, {d_csr_rowPtr, d_csr_colIdx, d_csr_rowIdx_zip, d_csr_val});
     }
     d_csr_zip(const d_csr_zip &) = delete;
     d_csr_zip &operator=(const d_csr_zip &) = delete;
     ~d_csr_zip()
     {
+        cola_compat::forget_holder(true, this);
         cudaFree(d_csr_rowPtr);
         cudaFree(d_csr_colIdx);
         cudaFree(d_csr_rowIdx_zip);
@@ -183,6 +283,13 @@ void ppl0_batch_SpMM(float *output, const float *input, const int *csr_rowPtr_l,
                      const int remote_col_num, const int dim, const int nodesPerPE, const int peid,
                      cudaStream_t stream)
 {
+    if (cola_zip_rows *h = cola_compat::cached_row_view(csr_rowPtr_l, csr_colIdx_l, csr_rowIdx_zip_l, csr_val_l,
+                                                        csc_colPtr_r, csc_rowIdx_r, csc_colIdx_zip_r, csc_val_r,
+                                                        local_row_lb, remote_col_lb, local_row_num, remote_col_num,
+                                                        nodesPerPE, peid, stream)) {
+        cola_compat::check(cola_zip_rows_spmm(h, output, input, dim, (cola_stream_t)stream), "ppl0_batch_SpMM");
+        return;
+    }
     cola_compat::check(cola_ppl0_batch_spmm(output, input, csr_rowPtr_l, csr_colIdx_l, csr_rowIdx_zip_l, csr_val_l,
                                             csc_colPtr_r, csc_rowIdx_r, csc_colIdx_zip_r, csc_val_r, local_row_lb,
                                             remote_col_lb, local_row_num, remote_col_num, dim, nodesPerPE, peid,

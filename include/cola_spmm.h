@@ -242,7 +242,8 @@ cola_status cola_ppl0_batch_buffer_spmm(float *output, const float *input, float
  * Limit: remote_col_num * dim must not exceed COLA_NOALLOC_STAGE_FLOATS;
  * larger requests return COLA_ERROR_INVALID_ARGUMENT and launch nothing.
  * The first call on a device looks up the array's device address (once per
- * device); make that first call before any stream capture.  All calls share
+ * device, and again after that device's context was reset, e.g. by
+ * cudaDeviceReset); make that first call before any stream capture.  All calls share
  * the one array: calls that overlap on the GPU (on different streams, or from
  * different threads) race on it and must be serialised by the caller.  The
  * array keeps whatever the last call left in it; every call overwrites the
@@ -254,6 +255,36 @@ cola_status cola_ppl0_batch_buffer_spmm_noalloc(float *output, const float *inpu
                                                 const float *csc_val_r, int32_t local_row_lb, int32_t remote_col_lb,
                                                 int32_t local_row_num, int32_t remote_col_num, int32_t dim,
                                                 int32_t nodesPerPE, int32_t peid, cola_stream_t stream);
+
+/* The row view of the chunks one ppl0_batch_SpMM call covers
+ * (include/dist_spmm_ppl_batch.cuh:202-245, the arguments of
+ * cola_ppl0_batch_spmm without the dense ones): the local CSR chunks
+ * [local_row_lb, +local_row_num) and remote CSC chunks [remote_col_lb,
+ * +remote_col_num) of PE peid, merged per output row in column order on the
+ * device (rows of more than 256 entries split into segments).  Built once
+ * (synchronises `stream`; needs about 12 bytes of device memory per entry
+ * while it runs and keeps about 8 per entry); the zip arrays are not read
+ * again.  cola_zip_rows_spmm then adds the same product as
+ * cola_ppl0_batch_spmm to `output` with the row-major schedule: one writer
+ * per row, no atomics, the same bits on every call.  compat.h's
+ * ppl0_batch_SpMM builds and keeps one for every d_csr_zip / d_csc_zip pair
+ * it is called with. */
+typedef struct cola_zip_rows cola_zip_rows;
+cola_status cola_zip_rows_create(const int32_t *csr_rowPtr_l, const int32_t *csr_colIdx_l,
+                                 const int32_t *csr_rowIdx_zip_l, const float *csr_val_l, const int32_t *csc_colPtr_r,
+                                 const int32_t *csc_rowIdx_r, const int32_t *csc_colIdx_zip_r, const float *csc_val_r,
+                                 int32_t local_row_lb, int32_t remote_col_lb, int32_t local_row_num,
+                                 int32_t remote_col_num, int32_t nodesPerPE, int32_t peid, cola_stream_t stream,
+                                 cola_zip_rows **out);
+/* output[r] += sum of the covered entries of row r times input rows (input =
+ * PE peid's slice of the symmetric X, as for cola_ppl0_batch_spmm); FP32,
+ * any dim >= 1.  Asynchronous on `stream`. */
+cola_status cola_zip_rows_spmm(cola_zip_rows *h, float *output, const float *input, int32_t dim,
+                               cola_stream_t stream);
+cola_status cola_zip_rows_free(cola_zip_rows *h);
+/* Rows spanned (up to the last with an entry), entries, hub rows, device bytes held. */
+cola_status cola_zip_rows_get_info(const cola_zip_rows *h, int64_t *rows, int64_t *nnz, int64_t *hub_rows,
+                                   int64_t *device_bytes);
 
 /* ppl_batch_SpMM (include/dist_spmm_ppl_batch.cuh:709-760): stage-i CSC
  * scatter over remote chunks [remote_col_lb, remote_col_ub).  Chunks in

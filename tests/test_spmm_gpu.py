@@ -529,3 +529,69 @@ def test_bulk_gather_wait_limit_reports_and_drains():
         cb.lib().cola_set_gather_wait_limit(0)
         cb.lib().cola_set_gather_bulk(0)
     assert cb.lib().cola_set_gather_wait_limit(-1) == 1  # COLA_ERROR_INVALID_ARGUMENT
+
+
+def _zip_rows(g, p, P):
+    z = g.zip_view(p)
+    h = ctypes.c_void_p()
+    args = [z.csr_rowPtr, z.csr_colIdx, z.csr_rowIdx_zip, z.csr_val, z.csc_colPtr, z.csc_rowIdx, z.csc_colIdx_zip,
+            z.csc_val]
+    args = [a if a is None or isinstance(a, ctypes.c_void_p) else ctypes.c_void_p(a) for a in args]
+    cb._lib.check(cb.lib().cola_zip_rows_create(*args, 0, 0, z.local_chunks, z.remote_chunks, g.nodes_per_part, p,
+                                                None, ctypes.byref(h)))
+    return h
+
+
+@pytest.mark.parametrize("K", [16, 100, 128, 256])
+def test_zip_rows_view_matches_reference_kernels_and_rows(K):
+    """The row view built from a PE's split blocks (what compat.h's
+    ppl0_batch_SpMM keeps per d_csr_zip / d_csc_zip pair) adds the same
+    product as the chunk launcher: within 1e-5 of FP64 and of the reference's
+    kernels, equal to the graph's own row-major output for the partition's
+    rows (the same entries in the same order; bit for bit where one lane group
+    takes a row), the same bits on a repeated call, and exactly twice that
+    after two calls into one output."""
+    P = 4
+    n, row, col, val, ps = graph_case(12, 16, seed=21, nparts=P)
+    g = S.Graph(ps)
+    npp = g.nodes_per_part
+    X = _padded_x(n, P, npp, K, seed=K)
+    Xd = torch.from_numpy(X).to(DEV)
+    ref64 = fp64_reference(n, row, col, val, X[:n])
+    rows = g.spmm(Xd[:n], schedule=S.SCHEDULE_ROWS)
+    L = cb.lib()
+    hs = [_zip_rows(g, p, P) for p in range(P)]
+    try:
+        outs = []
+        for rep in range(2):
+            Y = torch.zeros((P * npp, K), device=DEV)
+            for p in range(P):
+                cb._lib.check(L.cola_zip_rows_spmm(hs[p], ptr(Y[p * npp:]), ptr(Xd[p * npp:]), K, None))
+            torch.cuda.synchronize()
+            outs.append(Y)
+        Y2 = outs[1].clone()
+        for p in range(P):
+            cb._lib.check(L.cola_zip_rows_spmm(hs[p], ptr(Y2[p * npp:]), ptr(Xd[p * npp:]), K, None))
+        torch.cuda.synchronize()
+        nnz = ctypes.c_int64()
+        cb._lib.check(L.cola_zip_rows_get_info(hs[0], None, ctypes.byref(nnz), None, None))
+        z0 = g.zip_view(0)
+        assert nnz.value == z0.nnz_l + z0.nnz_r
+    finally:
+        for h in hs:
+            L.cola_zip_rows_free(h)
+    y = outs[0][:n]
+    assert rel(y.cpu().numpy(), ref64) <= TOL_F32
+    assert torch.equal(outs[0], outs[1])
+    if K // 4 > 16:
+        # one lane group per row (K > 64 FP32): each element is one FMA chain
+        # in column order, whichever tasks the rows fall in
+        assert torch.equal(y, rows)  # value equality (+0 and -0 compare equal)
+    else:
+        # narrower rows share a warp between lane groups, whose split of a row
+        # follows the row's offset in its task: the same sum in another order
+        assert rel(y.cpu().numpy(), rows.cpu().numpy()) <= 1e-6
+    assert torch.equal(Y2, 2 * outs[0])
+    if oracle.ref_available():
+        theirs = _run_reference(g, Xd, npp, K, P)[:n].cpu().numpy()
+        assert rel(y.cpu().numpy(), theirs) <= TOL_F32
