@@ -125,6 +125,25 @@ class Graph:
                               ctypes.byref(o), _stream(stream)))
         return Y
 
+    def autotune(self, X, Y=None, out_dtype=None, schedule=SCHEDULE_AUTO, reps=5, cache_path=None, stream=None):
+        """cola_spmm_autotune on these operands: returns (options dict for
+        spmm(), best ms, whether it came from the cache file)."""
+        _dense(X, "X")
+        K = X.shape[1]
+        if Y is None:
+            Y = torch.empty((self.num_nodes, K), dtype=out_dtype or torch.float32, device=X.device)
+        _dense(Y, "Y")
+        o = SpmmOpts()
+        ms = ctypes.c_float()
+        hit = ctypes.c_int32()
+        check(lib().cola_spmm_autotune(self._h, _ptr(X), _DT[X.dtype], X.stride(0), _ptr(Y), _DT[Y.dtype],
+                                       Y.stride(0), K, int(schedule), int(reps),
+                                       None if cache_path is None else str(cache_path).encode(), _stream(stream),
+                                       ctypes.byref(o), ctypes.byref(ms), ctypes.byref(hit)))
+        opts = dict(schedule=o.schedule, k_tile=o.k_tile, unroll=o.unroll, min_blocks=o.min_blocks,
+                    gather_batch_rows=o.gather_batch_rows)
+        return opts, ms.value, bool(hit.value)
+
     def close(self):
         if self._h is not None and self._h.value:
             lib().cola_graph_free(self._h)

@@ -420,6 +420,23 @@ typedef struct cola_spmm_opts {
 cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype x_dtype, int64_t ldx, void *Y, cola_dtype y_dtype,
                       int64_t ldy, int32_t K, const cola_spmm_opts *opts, cola_stream_t stream);
 
+/* The project's autotuner for one graph: times every candidate launch option
+ * of `schedule` (AUTO picks as cola_spmm does) on these operands with CUDA
+ * events, `reps` runs each after a warm-up, and returns the fastest in *best
+ * (schedule, k_tile, unroll, min_blocks, gather_batch_rows; accumulate 0).
+ * Row-major schedule: feature tile per pass x loads in flight x resident
+ * blocks per SM; for K >= 128 (FP32 X) or >= 256 (BF16 X) every candidate
+ * gives the same bits, narrower K has a single geometry.  Buffer and pipelined
+ * schedules: the remote-row gather batch (1,024 to 16,384 rows).  Y is
+ * overwritten; synchronises `stream`.  cache_path (may be NULL): a text file
+ * of tuned results keyed by device model, SM count, graph shape, K, dtypes and
+ * schedule; a hit returns its line without timing anything (*from_cache = 1),
+ * a miss appends one. */
+cola_status cola_spmm_autotune(cola_graph *g, const void *X, cola_dtype x_dtype, int64_t ldx, void *Y,
+                               cola_dtype y_dtype, int64_t ldy, int32_t K, int32_t schedule, int32_t reps,
+                               const char *cache_path, cola_stream_t stream, cola_spmm_opts *best, float *best_ms,
+                               int32_t *from_cache);
+
 /* ========================================================================
  * Batched form: many graphs of uneven size, each with its own X, Y and
  * feature width, in one persistent launch (plus one for hub rows).

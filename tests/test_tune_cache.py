@@ -1,7 +1,8 @@
-"""The batched autotuner's cache file (cola_b200/csrc/tune_cache.h), compiled on
-the CPU: a missing file or key misses, an appended line is found again, the
-first valid line for a key wins, and lines that do not parse or hold values
-outside the launch's search space are skipped."""
+"""The autotuners' cache file (cola_b200/csrc/tune_cache.h), compiled on the
+CPU: a missing file or key misses, an appended line is found again, the first
+valid line for a key wins, and lines that do not parse or hold values outside
+the launch's search space are skipped -- for the batched tuner's lines and the
+single-graph tuner's, which share a file without mixing."""
 import os
 import subprocess
 
@@ -51,3 +52,25 @@ def test_first_valid_line_wins_and_bad_lines_are_skipped(exe, tmp_path):
 def test_append_to_unwritable_path_fails(exe, tmp_path):
     res = subprocess.run([exe, "append", str(tmp_path / "no_dir" / "tune.txt"), KEY, "4", "100", "3", "1"])
     assert res.returncode == 1
+
+
+SKEY = "spmm|NVIDIA_B200|148|00112233aabbccdd"
+
+
+def test_single_graph_lines_round_trip_and_validity(exe, tmp_path):
+    path = tmp_path / "tune.txt"
+    sf = lambda key=SKEY: subprocess.run([exe, "sfind", str(path), key], capture_output=True, text=True,
+                                         check=True).stdout.split()
+    assert sf() == ["miss"]
+    path.write_text("\n".join([
+        KEY + " 4 50 3 9.25",               # a batch line: never a single-graph hit
+        SKEY + " 96 4 4 0 1.0",             # 96 is not a feature tile
+        SKEY + " 128 3 4 0 1.0",            # unroll 3 is not an option
+        SKEY + " 128 4 9 0 1.0",            # 9 blocks per SM is not an option
+        SKEY + " 128 8 6 0",                # truncated
+    ]) + "\n")
+    assert sf() == ["miss"]
+    subprocess.run([exe, "sappend", str(path), SKEY, "128", "8", "6", "0", "4.5"], check=True)
+    subprocess.run([exe, "sappend", str(path), SKEY, "64", "4", "4", "0", "9.0"], check=True)
+    assert sf() == ["hit", "128", "8", "6", "0", "4.500000"]
+    assert find(exe, str(path)) == ["hit", "4", "50", "3", "9.250000"]  # the batch line still found
