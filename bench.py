@@ -1054,7 +1054,8 @@ def serving_leg(args, seconds):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     t0 = time.time()
     rng = np.random.Generator(np.random.Philox(5))
-    srv = Server(memory_budget=120 << 30, slots=4, max_group=16)
+    srv = Server(memory_budget=120 << 30, slots=4, max_group=16, small_mib=args.serve_small_mib,
+                 copy_chunk_mib=args.serve_chunk_mib)
     gn, gnnz = [], []
     for i in range(args.serve_graphs):
         scale = int(rng.integers(12, 21))
@@ -1117,24 +1118,29 @@ def serving_leg(args, seconds):
     clocks.start()
     plan = [draw() for _ in range(nreq)]
     gaps = rng.exponential(1.0 / rate, nreq)
-    reqs = []
-    t_sub = []
+    # per size class: latency from submission to the result in host memory,
+    # taken by a waiter thread per request as its wait returns (the server's
+    # own statistics cover all requests together)
+    import concurrent.futures as cf
+    lat = [0.0] * nreq
+
+    def waiter(i, r, t0):
+        r.wait(timeout_ms=WAIT_MS)
+        lat[i] = (time.perf_counter() - t0) * 1e3
+
+    futs = []
     ts = time.perf_counter()
     t_next = ts
-    for d, gap in zip(plan, gaps):
-        t_next += gap
-        delay = t_next - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        t_sub.append(time.perf_counter())
-        reqs.append(submit(*d))
-    # per size class: latency from submission to the result in host memory,
-    # taken on this thread as each wait returns (waits in submission order, so
-    # a request's time is an upper bound when an earlier one finished later)
-    lat = [0.0] * nreq
-    for i, r in enumerate(reqs):
-        r.wait(timeout_ms=WAIT_MS)
-        lat[i] = (time.perf_counter() - t_sub[i]) * 1e3
+    with cf.ThreadPoolExecutor(max_workers=64) as pool:
+        for i, (d, gap) in enumerate(zip(plan, gaps)):
+            t_next += gap
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            t0 = time.perf_counter()
+            futs.append(pool.submit(waiter, i, submit(*d), t0))
+        for f in futs:
+            f.result()
     wall = time.perf_counter() - ts
     clk = clocks.stop()
     st = srv.stats()
@@ -1158,6 +1164,7 @@ def serving_leg(args, seconds):
             "kernel_ms_mean": st["kernel_ms_mean"], "copy_out_ms_mean": st["copy_out_ms_mean"],
             "peak_device_bytes": st["peak_bytes"], "budget_bytes": st["budget"],
             "per_size_class": per_class, "open_loop_seconds": round(wall, 2),
+            "small_mib": args.serve_small_mib or 16, "copy_chunk_mib": args.serve_chunk_mib or 32,
             "served_GBps": B / wall / 1e9, "prep_seconds": round(t_prep, 1),
             "latency": "submit to result in pinned host memory"}, B, wall, nreq, h2d, clk
 
@@ -1380,6 +1387,9 @@ def main():
     ap.add_argument("--serve-load", type=float, default=0.7, help="serving: offered rate / saturation rate")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="serving: length of the open-loop phase")
     ap.add_argument("--serve-min-requests", type=int, default=100)
+    ap.add_argument("--serve-small-mib", type=int, default=0,
+                    help="serving: size-class threshold in MiB of copies (0 = library default 16, -1 = FIFO)")
+    ap.add_argument("--serve-chunk-mib", type=int, default=0, help="serving: copy piece size (0 = library default)")
     ap.add_argument("--batch-graphs", type=int, default=512, help="batched workload: number of graphs")
     ap.add_argument("--tune-cache", default=None, help="batched workload: autotuner cache file (tuned once per shape)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "buffer", "rows"])

@@ -366,13 +366,25 @@ static cola_status launch_block_t(const dev::BlockArgs &ba, const RowsLaunch &a,
 {
     using T = typename dev::ElemOf<TR>::T;
     constexpr int W = LG * NV * TR::E;
-    auto fn = dev::rowblock_spmm_kernel<TR, TY, LG, NV, UNROLL, VEC, MINB>;
-    // one grid sweeps the feature tiles one after another
     const int64_t ntile = (a.K + W - 1) / W;
-    const int64_t gx = grid_for((const void *)fn, (ba.nseg + ba.ntask) * ntile);
+    if constexpr (LG == 32) {
+        if (a.k_tile > 0 && ntile > 1) {
+            // a requested tile width: one grid sweeps the tiles one after another
+            auto fn = dev::rowblock_tiled_kernel<TR, TY, NV, UNROLL, MINB>;
+            const int64_t gx = grid_for((const void *)fn, (ba.nseg + ba.ntask) * ntile);
+            t_launches++;
+            fn<<<(unsigned)gx, dev::kThreads, 0, st>>>(ba, static_cast<const T *>(a.X), a.ldx,
+                                                       static_cast<TY *>(a.Y), a.ldy, a.K, a.accumulate);
+            COLA_CUDA(cudaGetLastError());
+            return COLA_SUCCESS;
+        }
+    }
+    auto fn = dev::rowblock_spmm_kernel<TR, TY, LG, NV, UNROLL, VEC, MINB>;
+    const int64_t gx = grid_for((const void *)fn, ba.nseg + ba.ntask);
     t_launches++;
-    fn<<<(unsigned)gx, dev::kThreads, 0, st>>>(ba, static_cast<const T *>(a.X), a.ldx, static_cast<TY *>(a.Y), a.ldy,
-                                               a.K, a.accumulate);
+    fn<<<dim3((unsigned)gx, (unsigned)ntile), dev::kThreads, 0, st>>>(ba, static_cast<const T *>(a.X), a.ldx,
+                                                                      static_cast<TY *>(a.Y), a.ldy, a.K,
+                                                                      a.accumulate);
     COLA_CUDA(cudaGetLastError());
     return COLA_SUCCESS;
 }

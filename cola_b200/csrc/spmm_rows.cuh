@@ -470,23 +470,36 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
     __shared__ int2 s_ent[kWarpsPerBlock][32];
     int2 *ent = s_ent[threadIdx.x >> 5];
     constexpr int W = LG * NV * TR::E;
+    const int k0 = blockIdx.y * W;
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
-    const int64_t w0 = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const int64_t total = ba.nseg + ba.ntask;
+    rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5),
+                                                  nwarps, total, X, ldx, Y, ldy, K, accumulate, k0, ent);
+}
+
+// The same schedule with the feature tiles one after another instead of side
+// by side (blockIdx.y): the grid sweeps every item of tile 0, then of tile 1,
+// ..., so the X columns being gathered at any moment are one tile wide.  Every
+// element's sum is the same chain of FMAs whichever tile width computes it
+// (one lane group per row: LG = 32).  A separate kernel, so that the default
+// one keeps its own register allocation.
+template <typename TR, typename TY, int NV, int UNROLL, int MINB = 1>
+__global__ void __launch_bounds__(kThreads, MINB) rowblock_tiled_kernel(const __grid_constant__ BlockArgs ba,
+                                                                        const typename ElemOf<TR>::T *__restrict__ X,
+                                                                        int64_t ldx, TY *__restrict__ Y, int64_t ldy,
+                                                                        int K, int accumulate)
+{
+    __shared__ int2 s_ent[kWarpsPerBlock][32];
+    int2 *ent = s_ent[threadIdx.x >> 5];
+    constexpr int W = 32 * NV * TR::E;
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
     const int64_t total = ba.nseg + ba.ntask;
     const int ntile = (K + W - 1) / W;
-    if (ntile == 1) {
-        rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, w0, nwarps, total, X, ldx, Y, ldy, K, accumulate, 0, ent);
-        return;
-    }
-    // Feature tiles one after another: the grid sweeps every item of tile 0,
-    // then of tile 1, ..., so the X columns being gathered at any moment are
-    // one tile wide (a smaller working set in L2).  Every element's sum is the
-    // same chain of FMAs whichever tile width computes it.
-    for (int64_t w = w0; w < total * ntile; w += nwarps) {
+    for (int64_t w = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); w < total * ntile; w += nwarps) {
         const int tile = (int)(w / total);
         const int64_t it = w - (int64_t)tile * total;
-        rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, it, 1, it + 1, X, ldx, Y, ldy, K, accumulate, tile * W,
-                                                      ent);
+        rowblock_items<TR, TY, 32, NV, UNROLL, true>(ba, it, 1, it + 1, X, ldx, Y, ldy, K, accumulate, tile * W,
+                                                     ent);
     }
 }
 
