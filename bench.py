@@ -372,6 +372,21 @@ def run_reference(args, w):
     return 0
 
 
+def gather_ceilings(stream):
+    """Measured row-gather ceilings of this GPU (cola_probe_gather): 512-byte
+    rows at random indices from a 48 MiB table (L2-resident) and from a 4 GiB
+    table (DRAM), GB/s."""
+    import ctypes
+
+    import cola_b200 as cb
+    out = {}
+    for name, tb in (("l2", 48 << 20), ("dram", 4 << 30)):
+        v = ctypes.c_double()
+        rc = cb.lib().cola_probe_gather(tb, 512, 1 << 25, 5, ctypes.c_void_p(stream.cuda_stream), ctypes.byref(v))
+        out[name] = v.value if rc == 0 else None
+    return out
+
+
 def spmm_kw(args):
     """Launch options of the row-major schedule given on the command line."""
     return dict(unroll=args.unroll, min_blocks=args.min_blocks, k_tile=args.k_tile)
@@ -567,6 +582,8 @@ def run_ours(args, w):
     phys = traffic if traffic is not None else compulsory
     achieved = phys / k_s / 1e9
     alg_achieved = B / k_s / 1e9
+    ceil = gather_ceilings(stream) if not overridden else {"l2": None, "dram": None}
+    gather_bytes = int(info.nnz) * K * s_x  # the X rows the entries name (the gathers)
     launches_per_step = int(g.get_info().last_launches)  # counted by the library
     line = {
         "metric": METRIC, "value": B * world / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world,
@@ -596,7 +613,16 @@ def run_ours(args, w):
                      "traffic_over_compulsory": None if traffic is None else traffic / float(compulsory),
                      # the per-nonzero row-gather model: one X row per entry, most of them L2 hits
                      "alg_bytes": B, "alg_achieved": alg_achieved, "alg_frac": alg_achieved / peak,
-                     "alg_frac_of_8TBs": alg_achieved / 8000.0},
+                     "alg_frac_of_8TBs": alg_achieved / 8000.0,
+                     # what bounds the kernel: its X-row gathers against this GPU's own measured
+                     # gather ceilings (512-byte rows at random indices, cola_probe_gather)
+                     "gather": {"bytes": gather_bytes, "achieved": gather_bytes / k_s / 1e9,
+                                "l2_ceiling": ceil["l2"], "dram_ceiling": ceil["dram"],
+                                "frac_of_l2_ceiling": None if not ceil["l2"] else
+                                gather_bytes / k_s / 1e9 / ceil["l2"],
+                                "unit": "GB/s",
+                                "note": "ceilings: 512-byte rows at random indices from a 48 MiB table (L2) and "
+                                        "a 4 GiB table (DRAM), 8 rows in flight per warp, one full wave"}},
         "e2e": None if e2e_ms is None else {
             "value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": n * K * s_x,
             "d2h_bytes_per_step": n * K * s_y, "ms_per_step": e2e_ms,

@@ -102,6 +102,7 @@ SIGNATURES = {
     "cola_partition_build_device": (I32, [I32, I64, P, P, P, I32, P, P]),
     "cola_set_gather_bulk": (I32, [I32]),
     "cola_set_gather_wait_limit": (I32, [I64]),
+    "cola_probe_gather": (I32, [I64, I32, I64, I32, P, P]),
     "cola_device_error_check": (I32, [P]),
     "cola_graph_build_device": (I32, [I32, I64, P, P, P, I32, P, P, P]),
     "cola_nnz_split_device": (I32, [P, I64, P, I64, P, P, I64, P, P]),
@@ -132,6 +133,7 @@ SIGNATURES = {
     "cola_graph_get_info": (I32, [P, P]),
     "cola_graph_zip_view": (I32, [P, I32, P]),
     "cola_spmm": (I32, [P, P, I32, I64, P, I32, I64, I32, P, P]),
+    "cola_graph_set_hot_columns": (I32, [P, I64, P, P]),
     "cola_spmm_autotune": (I32, [P, P, I32, I64, P, I32, I64, I32, I32, I32, ctypes.c_char_p, P, P, P, P]),
     "cola_batch_create": (I32, [P, I32, P, P, P]),
     "cola_batch_create_from_graphs": (I32, [P, I32, P]),

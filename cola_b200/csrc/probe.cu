@@ -1,0 +1,107 @@
+// Ceilings of the row gather the SpMM kernels are made of, measured on the
+// device they run on (cola_probe_gather): warps read whole rows of a table
+// (16-byte vector loads across the warp, `unroll` rows in flight per warp, a
+// persistent grid of one full wave) at pseudo-random row indices.  With a table
+// that fits in L2 the rows come from L2 (the ceiling of the SpMM's gathers,
+// most of which hit L2); with a table several times larger than L2 they come
+// from DRAM.  The sums are kept (one value per warp) so that no load is dead.
+#include <algorithm>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "common.h"
+#include "graph.h"
+
+namespace cola {
+namespace probe {
+
+__device__ __forceinline__ uint32_t mix32(uint64_t x)
+{
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return (uint32_t)x;
+}
+
+template <int UNROLL>
+__global__ void __launch_bounds__(256) gather_probe_kernel(const uint4 *__restrict__ table, int64_t rows,
+                                                           int row_vecs, int64_t gathers, uint64_t seed,
+                                                           float *__restrict__ sink)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int64_t nwarps = (int64_t)gridDim.x * 8;
+    uint32_t acc = 0;
+    for (int64_t g0 = warp * UNROLL; g0 < gathers; g0 += nwarps * UNROLL) {
+        uint4 v[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; u++) {
+            const int64_t r = (int64_t)(mix32(seed + (uint64_t)(g0 + u)) % (uint64_t)rows);
+            const uint4 *p = table + r * row_vecs;
+            v[u] = lane < row_vecs ? __ldg(p + lane) : make_uint4(0, 0, 0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; u++)
+            acc += v[u].x ^ v[u].y ^ v[u].z ^ v[u].w;
+    }
+    if (acc == 0x9e3779b9u)  // practically never: keeps the loads alive
+        sink[warp] = (float)acc;
+}
+
+}  // namespace probe
+}  // namespace cola
+
+using namespace cola;
+
+extern "C" cola_status cola_probe_gather(int64_t table_bytes, int32_t row_bytes, int64_t gathers, int32_t reps,
+                                         cola_stream_t stream, double *gbps)
+{
+    COLA_REQUIRE(gbps && table_bytes >= row_bytes && row_bytes >= 16 && row_bytes <= 512 && row_bytes % 16 == 0 &&
+                     gathers >= 1 && reps >= 1,
+                 COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_probe_gather: table %lld bytes, rows of %d bytes (16..512, a multiple of 16), %lld gathers",
+                 (long long)table_bytes, row_bytes, (long long)gathers);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t rows = table_bytes / row_bytes;
+    void *table = nullptr;
+    float *sink = nullptr;
+    const int blocks = sm_count() * blocks_per_sm((const void *)probe::gather_probe_kernel<8>, 256);
+    COLA_CUDA(cudaMallocAsync(&table, (size_t)(rows * row_bytes), st));
+    cudaError_t e = cudaMallocAsync((void **)&sink, (size_t)blocks * 8 * sizeof(float), st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(table, 0x5a, (size_t)(rows * row_bytes), st);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&e0);
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&e1);
+    float ms = 0.f;
+    for (int pass = 0; pass < 2 && e == cudaSuccess; pass++) {  // pass 0 warms the cache
+        e = cudaEventRecord(e0, st);
+        for (int r = 0; r < (pass ? reps : 1) && e == cudaSuccess; r++) {
+            probe::gather_probe_kernel<8><<<blocks, 256, 0, st>>>(static_cast<const uint4 *>(table), rows,
+                                                                  row_bytes / 16, gathers, 0x1234567ull + 977ull * r,
+                                                                  sink);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess)
+            e = cudaEventRecord(e1, st);
+        if (e == cudaSuccess)
+            e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess && pass)
+            e = cudaEventElapsedTime(&ms, e0, e1);
+    }
+    if (e0)
+        cudaEventDestroy(e0);
+    if (e1)
+        cudaEventDestroy(e1);
+    cudaFreeAsync(sink, st);
+    cudaFreeAsync(table, st);
+    COLA_CUDA(e);
+    COLA_CUDA(cudaStreamSynchronize(st));
+    *gbps = (double)gathers * row_bytes * reps / (ms * 1e-3) / 1e9;
+    return COLA_SUCCESS;
+}

@@ -341,6 +341,17 @@ cola_status cola_graph_build_device(int32_t num_nodes, int64_t nnz, const int32_
                                     cola_stream_t stream, cola_graph **out);
 
 
+/* Marks the graph's most referenced columns as hot: the row-major schedule then
+ * loads their X rows with an L2 evict-last policy and every other X row with
+ * evict-first, so that the rows reused most stay in L2 while the rest stream
+ * past (for the default feature tile, FP32 or BF16 X with K = 128 / 256, at 3
+ * or 4 blocks per SM; other launches ignore the marks).  The hot set is every
+ * column of degree >= d, for the smallest d that marks at most hot_columns
+ * columns (*marked receives the count); hot_columns = 0 clears the marks.  The
+ * marks are one bit per entry (nnz / 8 bytes, kept with the graph).  Results
+ * are the same bits either way.  Synchronises `stream`. */
+cola_status cola_graph_set_hot_columns(cola_graph *g, int64_t hot_columns, cola_stream_t stream, int64_t *marked);
+
 typedef struct cola_graph_info {
     int32_t num_nodes, nparts, nodes_per_part, group_size;
     int64_t nnz, nnz_local, nnz_remote;
@@ -365,6 +376,16 @@ cola_status cola_set_gather_bulk(int32_t enable);
  * issued; cola_device_error_check then reports it.  Small values exist to
  * exercise that path. */
 cola_status cola_set_gather_wait_limit(int64_t polls);
+
+/* The row-gather ceiling of the current device: warps read whole rows of
+ * row_bytes (16..512) from a table of table_bytes at pseudo-random row indices
+ * (16-byte loads, 8 rows in flight per warp, one full wave), `gathers` rows per
+ * run, `reps` timed runs after one warm-up run; *gbps = row bytes read per
+ * second.  A table that fits in L2 measures the L2 ceiling of the SpMM's
+ * gathers, a table far larger than L2 the DRAM ceiling.  Allocates the table
+ * (stream-ordered) and synchronises `stream`. */
+cola_status cola_probe_gather(int64_t table_bytes, int32_t row_bytes, int64_t gathers, int32_t reps,
+                              cola_stream_t stream, double *gbps);
 
 /* Waits for the current device, then reports (and clears) the error code a
  * kernel left when one of its bounded waits ran out: 0 = none; 1 = a bulk-copy
