@@ -374,13 +374,13 @@ def run_reference(args, w):
 
 def gather_ceilings(stream):
     """Measured row-gather ceilings of this GPU (cola_probe_gather): 512-byte
-    rows at random indices from a 48 MiB table (L2-resident) and from a 4 GiB
+    rows at random indices from a 16 MiB table (L2-resident) and from a 4 GiB
     table (DRAM), GB/s."""
     import ctypes
 
     import cola_b200 as cb
     out = {}
-    for name, tb in (("l2", 48 << 20), ("dram", 4 << 30)):
+    for name, tb in (("l2", 16 << 20), ("dram", 4 << 30)):
         v = ctypes.c_double()
         rc = cb.lib().cola_probe_gather(tb, 512, 1 << 25, 5, ctypes.c_void_p(stream.cuda_stream), ctypes.byref(v))
         out[name] = v.value if rc == 0 else None
@@ -621,7 +621,7 @@ def run_ours(args, w):
                                 "frac_of_l2_ceiling": None if not ceil["l2"] else
                                 gather_bytes / k_s / 1e9 / ceil["l2"],
                                 "unit": "GB/s",
-                                "note": "ceilings: 512-byte rows at random indices from a 48 MiB table (L2) and "
+                                "note": "ceilings: 512-byte rows at random indices from a 16 MiB table (L2) and "
                                         "a 4 GiB table (DRAM), 8 rows in flight per warp, one full wave"}},
         "e2e": None if e2e_ms is None else {
             "value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": n * K * s_x,

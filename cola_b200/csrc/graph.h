@@ -87,9 +87,6 @@ struct cola_graph {
     int32_t hub_threshold = 256, hub_segment = 256, task_entries = 256;
     float *ws_hub = nullptr;  // nseg x K partials
     size_t ws_hub_bytes = 0;
-    int64_t hot_columns = 0;      // columns marked hot (cola_graph_set_hot_columns; 0: none)
-    uint32_t *hot_bits = nullptr;  // one bit per row-view entry: its column is hot
-    size_t hot_bits_words = 0;
 };
 
 namespace cola {

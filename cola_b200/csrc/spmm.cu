@@ -297,7 +297,6 @@ struct RowsLaunch {
     int unroll;
     int min_blocks;
     int k_tile;
-    bool hot;  // the row view marks hot columns: loads with L2 eviction priorities
 };
 
 template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC>
@@ -362,7 +361,7 @@ static cola_status launch_rows(const RowsLaunch &a, cudaStream_t st)
                  : launch_rows_geo<dev::ScalarTraits<BF>, BF, false>(a, a.K, st);
 }
 
-template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC, int MINB = 1, bool HOT = false>
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC, int MINB = 1>
 static cola_status launch_block_t(const dev::BlockArgs &ba, const RowsLaunch &a, cudaStream_t st)
 {
     using T = typename dev::ElemOf<TR>::T;
@@ -380,7 +379,7 @@ static cola_status launch_block_t(const dev::BlockArgs &ba, const RowsLaunch &a,
             return COLA_SUCCESS;
         }
     }
-    auto fn = dev::rowblock_spmm_kernel<TR, TY, LG, NV, UNROLL, VEC, MINB, HOT>;
+    auto fn = dev::rowblock_spmm_kernel<TR, TY, LG, NV, UNROLL, VEC, MINB>;
     const int64_t gx = grid_for((const void *)fn, ba.nseg + ba.ntask);
     t_launches++;
     fn<<<dim3((unsigned)gx, (unsigned)ntile), dev::kThreads, 0, st>>>(ba, static_cast<const T *>(a.X), a.ldx,
@@ -434,12 +433,6 @@ static cola_status launch_block_geo(const dev::BlockArgs &ba, const RowsLaunch &
         // resident blocks per SM: measured best 3 for FP32 X (K = 128: 3 % faster
         // than 4) and 4 for BF16 X (5 % faster than 3)
         const int mb = a.min_blocks > 0 ? a.min_blocks : (TR::E == 4 ? 3 : 4);
-        if constexpr (std::is_same<TR, dev::VecTraits<float>>::value ||
-                      std::is_same<TR, dev::VecTraits<__nv_bfloat16>>::value) {
-            if (a.hot && a.k_tile == 0)  // the hot-column form: the default tile at 3 or 4 blocks per SM
-                return mb == 3 ? launch_block_t<TR, TY, 32, 1, 4, true, 3, true>(ba, a, st)
-                               : launch_block_t<TR, TY, 32, 1, 4, true, 4, true>(ba, a, st);
-        }
         if (mb == 3)
             return launch_block_t<TR, TY, 32, 1, 4, true, 3>(ba, a, st);
         if (mb == 5)
@@ -729,7 +722,6 @@ void graph_release(cola_graph *g)
     cudaFree(g->stage_buf);
     cudaFree(g->ws);
     cudaFree(g->ws_hub);
-    cudaFree(g->hot_bits);
     cudaSetDevice(cur);
     delete g;
 }
@@ -1094,114 +1086,6 @@ cola_status cola_set_gather_bulk(int32_t enable)
     return COLA_SUCCESS;
 }
 
-namespace cola {
-namespace hot {
-__global__ void degree_kernel(const int32_t *__restrict__ col, int64_t n, int32_t *__restrict__ deg)
-{
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(deg + col[i], 1);
-}
-__global__ void max_col_kernel(const int32_t *__restrict__ col, int64_t n, int32_t *__restrict__ out)
-{
-    int32_t m = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        m = max(m, col[i]);
-    atomicMax(out, m);
-}
-// word w of the mark bitmap: bit b set when entry 32w + b names a column of
-// degree >= thr
-__global__ void bits_kernel(const int32_t *__restrict__ col, int64_t n, const int32_t *__restrict__ deg, int32_t thr,
-                            uint32_t *__restrict__ bits)
-{
-    const int64_t words = (n + 31) / 32;
-    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t v = 0;
-        for (int b = 0; b < 32 && w * 32 + b < n; b++)
-            v |= (uint32_t)(deg[col[w * 32 + b]] >= thr) << b;
-        bits[w] = v;
-    }
-}
-}  // namespace hot
-}  // namespace cola
-
-cola_status cola_graph_set_hot_columns(cola_graph *g, int64_t hot_columns, cola_stream_t stream, int64_t *marked)
-{
-    COLA_REQUIRE(g && hot_columns >= 0, COLA_ERROR_INVALID_ARGUMENT, "cola_graph_set_hot_columns: bad argument");
-    COLA_REQUIRE(g->has_rows, COLA_ERROR_INVALID_ARGUMENT,
-                 "cola_graph_set_hot_columns: the graph has no row view");
-    cudaStream_t st = (cudaStream_t)stream;
-    const int64_t n = g->N > 0 ? g->N : 0;
-    int64_t nnz = 0;
-    COLA_CUDA(cudaMemcpyAsync(&nnz, g->rv_ptr + n, sizeof nnz, cudaMemcpyDeviceToHost, st));
-    COLA_CUDA(cudaStreamSynchronize(st));
-    // columns are global ids below N for an uploaded graph; a zip row view may
-    // name columns past its rows: the degree table is sized by the largest id
-    int32_t ncol = (int32_t)n;
-    int32_t *deg = nullptr;
-    const int32_t *col = g->rv_col;
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nnz + 255) / 256, (int64_t)sm_count() * 8));
-    int64_t count = 0;
-    if (nnz > 0) {
-        // the largest column id (hot bit cleared) bounds the degree table
-        int32_t maxc = 0;
-        {
-            int32_t *d_max = nullptr;
-            COLA_CUDA(cudaMallocAsync((void **)&d_max, sizeof(int32_t), st));
-            COLA_CUDA(cudaMemsetAsync(d_max, 0, sizeof(int32_t), st));
-            hot::max_col_kernel<<<blocks, 256, 0, st>>>(col, nnz, d_max);
-            COLA_CUDA(cudaMemcpyAsync(&maxc, d_max, sizeof maxc, cudaMemcpyDeviceToHost, st));
-            COLA_CUDA(cudaFreeAsync(d_max, st));
-            COLA_CUDA(cudaStreamSynchronize(st));
-        }
-        ncol = std::max<int32_t>(ncol, maxc + 1);
-        COLA_CUDA(cudaMallocAsync((void **)&deg, (size_t)ncol * sizeof(int32_t), st));
-        COLA_CUDA(cudaMemsetAsync(deg, 0, (size_t)ncol * sizeof(int32_t), st));
-        hot::degree_kernel<<<blocks, 256, 0, st>>>(col, nnz, deg);
-        std::vector<int32_t> h((size_t)ncol);
-        COLA_CUDA(cudaMemcpyAsync(h.data(), deg, (size_t)ncol * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-        COLA_CUDA(cudaStreamSynchronize(st));
-        // the smallest degree threshold that marks at most hot_columns columns
-        int32_t thr = 0;
-        if (hot_columns > 0) {
-            int32_t dmax = 0;
-            for (int32_t d : h)
-                dmax = std::max(dmax, d);
-            std::vector<int64_t> by((size_t)dmax + 2, 0);
-            for (int32_t d : h)
-                by[(size_t)d]++;
-            int64_t acc = 0;
-            thr = dmax + 1;
-            for (int32_t d = dmax; d >= 1; d--) {
-                if (acc + by[(size_t)d] > hot_columns)
-                    break;
-                acc += by[(size_t)d];
-                thr = d;
-            }
-            count = acc;
-            if (count == 0)
-                thr = 0;
-        }
-        if (count > 0) {
-            const size_t words = (size_t)((nnz + 31) / 32);
-            if (g->hot_bits_words < words) {
-                cudaFree(g->hot_bits);
-                g->hot_bits = nullptr;
-                g->hot_bits_words = 0;
-                COLA_CUDA(cudaMalloc((void **)&g->hot_bits, words * 4));
-                g->hot_bits_words = words;
-            }
-            hot::bits_kernel<<<blocks, 256, 0, st>>>(col, nnz, deg, thr, g->hot_bits);
-            COLA_CUDA(cudaGetLastError());
-        }
-        COLA_CUDA(cudaFreeAsync(deg, st));
-        COLA_CUDA(cudaStreamSynchronize(st));
-    }
-    g->hot_columns = count;
-    if (marked)
-        *marked = count;
-    return COLA_SUCCESS;
-}
-
 cola_status cola_set_gather_wait_limit(int64_t polls)
 {
     COLA_REQUIRE(polls >= 0 && polls <= (int64_t)dev::kWaitLimitDefault * 64, COLA_ERROR_INVALID_ARGUMENT,
@@ -1294,9 +1178,8 @@ static cola_status spmm_impl(cola_graph *g, const void *X, cola_dtype xdt, int64
         a.unroll = opts ? opts->unroll : 0;
         a.min_blocks = opts ? opts->min_blocks : 0;
         a.k_tile = opts ? opts->k_tile : 0;
-        a.hot = g->hot_columns > 0 && g->hot_bits;
         if (a.vec) {
-            dev::BlockArgs ba = {};
+            dev::BlockArgs ba;
             ba.rowptr = g->rv_ptr;
             ba.col = g->rv_col;
             ba.val = g->rv_val;
@@ -1309,7 +1192,6 @@ static cola_status spmm_impl(cola_graph *g, const void *X, cola_dtype xdt, int64
             ba.seg_len = g->hub_segment;
             ba.ws = g->ws_hub;
             ba.ld_ws = K;
-            ba.hot_bits = g->hot_columns > 0 ? g->hot_bits : nullptr;
             COLA_TRY(launch_block(ba, a, st));
         } else {
             COLA_TRY(launch_rows(a, st));

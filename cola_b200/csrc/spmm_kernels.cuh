@@ -51,40 +51,11 @@ struct PartDesc {
 template <typename T>
 struct VecTraits;
 
-// L2 eviction-priority policies (createpolicy) for the hinted loads below.
-__device__ __forceinline__ uint64_t l2_policy_evict_last()
-{
-    uint64_t pol;
-    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-__device__ __forceinline__ uint64_t l2_policy_evict_first()
-{
-    uint64_t pol;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-
-__device__ __forceinline__ uint4 ldg_hint_u4(const void *p, uint64_t pol)
-{
-    uint4 v;
-    asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                 : "l"(p), "l"(pol));
-    return v;
-}
-
 template <>
 struct VecTraits<float> {
     static constexpr int E = 4;
     using raw_t = float4;
     __device__ __forceinline__ static raw_t load(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
-    // the same load with an L2 eviction-priority policy
-    __device__ __forceinline__ static raw_t load_hint(const float *p, uint64_t pol)
-    {
-        const uint4 v = ldg_hint_u4(p, pol);
-        return make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w));
-    }
     __device__ __forceinline__ static raw_t zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
     __device__ __forceinline__ static void unpack(const raw_t &r, float (&f)[E])
     {
@@ -102,10 +73,6 @@ struct VecTraits<__nv_bfloat16> {
     __device__ __forceinline__ static raw_t load(const __nv_bfloat16 *p)
     {
         return __ldg(reinterpret_cast<const uint4 *>(p));
-    }
-    __device__ __forceinline__ static raw_t load_hint(const __nv_bfloat16 *p, uint64_t pol)
-    {
-        return ldg_hint_u4(p, pol);
     }
     __device__ __forceinline__ static raw_t zero() { return make_uint4(0u, 0u, 0u, 0u); }
     // BF16 -> FP32 is exact: the 16 bits become the high half of the float.

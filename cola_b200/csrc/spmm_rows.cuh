@@ -16,13 +16,6 @@
 namespace cola {
 namespace dev {
 
-// Hot columns (cola_graph_set_hot_columns): one bit per row-view entry
-// (BlockArgs::hot_bits) marks an entry whose column is among the most
-// referenced; the kernel built for it (HOT) loads those X rows with an L2
-// evict-last policy and every other X row with evict-first.  Inside that
-// kernel the mark travels as the top bit of the entry's column field.
-constexpr int32_t kColMask = 0x7fffffff;
-
 // Store E accumulated values to Y (FP32 or BF16), optionally adding the old
 // contents (single writer, so a plain read-modify-write).
 template <typename TY, int E, bool VEC_Y>
@@ -248,7 +241,6 @@ struct BlockArgs {
     int32_t seg_len;
     float *ws;
     int64_t ld_ws;
-    const uint32_t *hot_bits;  // entry e is hot when bit e % 32 of word e / 32 is set (HOT kernels)
 };
 
 // acc[q] += v * x[2q .. 2q+1] for one 16-byte vector of X, with the packed
@@ -281,8 +273,7 @@ __device__ __forceinline__ void fma_vec2(float2 (&acc)[TR::E / 2], float v, cons
 // BARef is `const BlockArgs` (the single-graph kernel: arguments read straight
 // from the kernel's parameter space) or `const BlockArgs &` (the batched form:
 // a descriptor in global memory).
-template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, typename BARef = const BlockArgs,
-          bool HOT = false>
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, typename BARef = const BlockArgs>
 __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, const int64_t stride,
                                                const int64_t total,
                                               const typename ElemOf<TR>::T *__restrict__ X, const int64_t ldx,
@@ -304,11 +295,6 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
     for (int j = 0; j < NV; j++)
         kok[j] = (k0 + (gl + j * lg) * E) < K;
     const T *xk = X + k0 + gl * E;
-    uint64_t pol_hot = 0, pol_cold = 0;
-    if constexpr (HOT) {
-        pol_hot = l2_policy_evict_last();
-        pol_cold = l2_policy_evict_first();
-    }
 
     for (int64_t it = it0; it < total; it += stride) {
         const bool seg = it < ba.nseg;
@@ -400,10 +386,6 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
             // the entry stream is read once: evict-first, so it does not push X rows out of L2
             mc = __ldcs(colp + lane);
             mv = __ldcs(valp + lane);
-            if constexpr (HOT) {  // the entry's hot mark, as the top bit of its column field
-                const int64_t e = e_beg + lane;
-                mc |= (int32_t)(((__ldg(ba.hot_bits + (e >> 5)) >> (e & 31)) & 1u) << 31);
-            }
         }
         for (int32_t base = 0; base < n_ent; base += 32) {
             const int n = min(32, n_ent - base);
@@ -414,10 +396,6 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
             if (base + 32 + lane < n_ent) {
                 mc = __ldcs(colp + base + 32 + lane);
                 mv = __ldcs(valp + base + 32 + lane);
-                if constexpr (HOT) {
-                    const int64_t e = e_beg + base + 32 + lane;
-                    mc |= (int32_t)(((__ldg(ba.hot_bits + (e >> 5)) >> (e & 31)) & 1u) << 31);
-                }
             }
             for (int jj = 0; jj < n; jj += R) {
                 raw_t xr[UNROLL][NV];
@@ -428,20 +406,11 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
                     for (int u = 0; u < UNROLL; u++) {
                         const int2 p = ent[jj + u * G + g];
                         vv[u] = __int_as_float(p.y);
-                        if constexpr (HOT) {
-                            const T *xp = xk + (int64_t)(p.x & kColMask) * ldx;
-                            const uint64_t pol = p.x < 0 ? pol_hot : pol_cold;
+                        const T *xp = xk + (int64_t)p.x * ldx;
     #pragma unroll
-                            for (int j = 0; j < NV; j++)
-                                if (kok[j])
-                                    xr[u][j] = TR::load_hint(xp + j * lg * E, pol);
-                        } else {
-                            const T *xp = xk + (int64_t)p.x * ldx;
-    #pragma unroll
-                            for (int j = 0; j < NV; j++)
-                                if (kok[j])
-                                    xr[u][j] = TR::load(xp + j * lg * E);
-                        }
+                        for (int j = 0; j < NV; j++)
+                            if (kok[j])
+                                xr[u][j] = TR::load(xp + j * lg * E);
                     }
     #pragma unroll
                     for (int u = 0; u < UNROLL; u++)
@@ -455,20 +424,11 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
                         if (idx < n) {
                             const int2 p = ent[idx];
                             vv[u] = __int_as_float(p.y);
-                            if constexpr (HOT) {
-                                const T *xp = xk + (int64_t)(p.x & kColMask) * ldx;
-                                const uint64_t pol = p.x < 0 ? pol_hot : pol_cold;
+                            const T *xp = xk + (int64_t)p.x * ldx;
     #pragma unroll
-                                for (int j = 0; j < NV; j++)
-                                    if (kok[j])
-                                        xr[u][j] = TR::load_hint(xp + j * lg * E, pol);
-                            } else {
-                                const T *xp = xk + (int64_t)p.x * ldx;
-    #pragma unroll
-                                for (int j = 0; j < NV; j++)
-                                    if (kok[j])
-                                        xr[u][j] = TR::load(xp + j * lg * E);
-                            }
+                            for (int j = 0; j < NV; j++)
+                                if (kok[j])
+                                    xr[u][j] = TR::load(xp + j * lg * E);
                         }
                     }
                     // cut the round [lo, hi) at the row ends it contains
@@ -499,7 +459,7 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
     }
 }
 
-template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, int MINB = 1, bool HOT = false>
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, int MINB = 1>
 __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __grid_constant__ BlockArgs ba,
                                                                        const typename ElemOf<TR>::T *__restrict__ X,
                                                                        int64_t ldx, TY *__restrict__ Y, int64_t ldy,
@@ -513,9 +473,8 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
     const int k0 = blockIdx.y * W;
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
     const int64_t total = ba.nseg + ba.ntask;
-    rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y, const BlockArgs, HOT>(
-        ba, (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5), nwarps, total, X, ldx, Y, ldy, K, accumulate,
-        k0, ent);
+    rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5),
+                                                  nwarps, total, X, ldx, Y, ldy, K, accumulate, k0, ent);
 }
 
 // The same schedule with the feature tiles one after another instead of side

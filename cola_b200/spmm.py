@@ -125,14 +125,6 @@ class Graph:
                               ctypes.byref(o), _stream(stream)))
         return Y
 
-    def set_hot_columns(self, hot_columns, stream=None):
-        """cola_graph_set_hot_columns: mark at most `hot_columns` most
-        referenced columns for L2 evict-last loads (0 clears); returns the
-        number marked."""
-        m = ctypes.c_int64()
-        check(lib().cola_graph_set_hot_columns(self._h, int(hot_columns), _stream(stream), ctypes.byref(m)))
-        return m.value
-
     def autotune(self, X, Y=None, out_dtype=None, schedule=SCHEDULE_AUTO, reps=5, cache_path=None, stream=None):
         """cola_spmm_autotune on these operands: returns (options dict for
         spmm(), best ms, whether it came from the cache file)."""

@@ -341,17 +341,6 @@ cola_status cola_graph_build_device(int32_t num_nodes, int64_t nnz, const int32_
                                     cola_stream_t stream, cola_graph **out);
 
 
-/* Marks the graph's most referenced columns as hot: the row-major schedule then
- * loads their X rows with an L2 evict-last policy and every other X row with
- * evict-first, so that the rows reused most stay in L2 while the rest stream
- * past (for the default feature tile, FP32 or BF16 X with K = 128 / 256, at 3
- * or 4 blocks per SM; other launches ignore the marks).  The hot set is every
- * column of degree >= d, for the smallest d that marks at most hot_columns
- * columns (*marked receives the count); hot_columns = 0 clears the marks.  The
- * marks are one bit per entry (nnz / 8 bytes, kept with the graph).  Results
- * are the same bits either way.  Synchronises `stream`. */
-cola_status cola_graph_set_hot_columns(cola_graph *g, int64_t hot_columns, cola_stream_t stream, int64_t *marked);
-
 typedef struct cola_graph_info {
     int32_t num_nodes, nparts, nodes_per_part, group_size;
     int64_t nnz, nnz_local, nnz_remote;

@@ -595,26 +595,3 @@ def test_zip_rows_view_matches_reference_kernels_and_rows(K):
     if oracle.ref_available():
         theirs = _run_reference(g, Xd, npp, K, P)[:n].cpu().numpy()
         assert rel(y.cpu().numpy(), theirs) <= TOL_F32
-
-
-@pytest.mark.parametrize("K,xdt,ydt", [(128, torch.float32, torch.float32), (256, torch.bfloat16, torch.bfloat16),
-                                       (256, torch.float32, torch.bfloat16)])
-def test_hot_columns_same_bits(case12, K, xdt, ydt):
-    """Marking the most referenced columns (L2 evict-last loads for their X
-    rows, evict-first for the rest) changes where rows are cached, not what
-    is summed: the same bits with and without marks, at both occupancies,
-    and after the marks are cleared."""
-    n, row, col, val, ps = case12
-    g = S.Graph(ps, hub_threshold=32, hub_segment=16)
-    X = torch.from_numpy(dense_x(n, K, seed=K)).to(DEV).to(xdt)
-    base = g.spmm(X, out_dtype=ydt)
-    deg = np.bincount(col, minlength=n)
-    marked = g.set_hot_columns(300)
-    assert 0 < marked <= 300
-    thr = np.sort(deg)[::-1][marked - 1]
-    assert np.count_nonzero(deg >= thr) == marked  # every column of degree >= d, for one d
-    for mb in (3, 4):
-        y = g.spmm(X, out_dtype=ydt, min_blocks=mb)
-        assert torch.equal(y.float(), base.float()) and torch.equal(y, base)
-    assert g.set_hot_columns(0) == 0
-    assert torch.equal(g.spmm(X, out_dtype=ydt), base)
