@@ -622,7 +622,7 @@ def run_ours(args, w):
                                 gather_bytes / k_s / 1e9 / ceil["l2"],
                                 "unit": "GB/s",
                                 "note": "ceilings: 512-byte rows at random indices from a 16 MiB table (L2) and "
-                                        "a 4 GiB table (DRAM), 8 rows in flight per warp, one full wave"}},
+                                        "a 4 GiB table (DRAM), 4 rows in flight per warp, one full wave"}},
         "e2e": None if e2e_ms is None else {
             "value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": n * K * s_x,
             "d2h_bytes_per_step": n * K * s_y, "ms_per_step": e2e_ms,
@@ -847,15 +847,42 @@ def reference_kernels_baseline(g, X, n, K, P, B, k_ms, stream, steps=10):
             total += a.elapsed_time(b)
         return total
 
+    # one row view of every PE's chunks (what compat.h's distSpMM_ppl_batch_all keeps for
+    # a single stage): one call per SpMM
+    parts = (cb._lib.ZipPart * P)()
+    for p, z in enumerate(zips):
+        q = parts[p]
+        q.csr_rowPtr_l, q.csr_colIdx_l, q.csr_rowIdx_zip_l, q.csr_val_l = (z.csr_rowPtr, z.csr_colIdx,
+                                                                           z.csr_rowIdx_zip, z.csr_val)
+        q.csc_colPtr_r, q.csc_rowIdx_r, q.csc_colIdx_zip_r, q.csc_val_r = (z.csc_colPtr, z.csc_rowIdx,
+                                                                           z.csc_colIdx_zip, z.csc_val)
+        q.local_row_lb, q.remote_col_lb, q.local_row_num, q.remote_col_num = 0, 0, z.local_chunks, z.remote_chunks
+    hall = ctypes.c_void_p()
+    if L.cola_zip_rows_create_all(parts, P, npp, sh, ctypes.byref(hall)) != 0:
+        raise RuntimeError("cola_zip_rows_create_all failed")
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def spmm_all():
+        ea.record(stream)
+        rc = L.cola_zip_rows_spmm(hall, ctypes.c_void_p(Yr.data_ptr()), ctypes.c_void_p(Xr.data_ptr()), K, sh)
+        eb.record(stream)
+        if rc != 0:
+            raise RuntimeError("cola_zip_rows_spmm failed")
+        torch.cuda.synchronize()
+        return ea.elapsed_time(eb)
+
     for _ in range(3):
         spmm()
         spmm(True)
         spmm_views()
+        spmm_all()
     ms = sum(spmm() for _ in range(steps)) / steps
     ours_kl = sum(spmm(True) for _ in range(steps)) / steps
     ours_rv = sum(spmm_views() for _ in range(steps)) / steps
+    ours_all = sum(spmm_all() for _ in range(steps)) / steps
     for h in views:
         L.cola_zip_rows_free(h)
+    L.cola_zip_rows_free(hall)
     del Xr, Yr
     return {"ms_per_spmm": ms, "value": B / (ms * 1e-3) / 1e9, "unit": "GB/s",
             "kernel": "ppl0_batch_SpMM<{}, {}> per virtual partition (include/dist_spmm_ppl_batch.cuh:76-245), "
@@ -866,7 +893,9 @@ def reference_kernels_baseline(g, X, n, K, P, B, k_ms, stream, steps=10):
             "ours_kernel_level_ms_per_spmm": ours_kl, "ours_kernel_level_speedup": ms / ours_kl,
             # the same per-PE calls on the row view of each PE's zip arrays (built once), as
             # compat.h's ppl0_batch_SpMM / distSpMM_ppl_batch_wrapper run them
-            "ours_row_view_ms_per_spmm": ours_rv, "ours_row_view_speedup": ms / ours_rv}
+            "ours_row_view_ms_per_spmm": ours_rv, "ours_row_view_speedup": ms / ours_rv,
+            # all PEs' chunks in one row view (compat.h distSpMM_ppl_batch_all, single stage)
+            "ours_all_pes_row_view_ms_per_spmm": ours_all, "ours_all_pes_row_view_speedup": ms / ours_all}
 
 
 def make_batched(count, seed):

@@ -75,6 +75,12 @@ class BatchInfo(ctypes.Structure):
                 ("last_launches", I64)]
 
 
+class ZipPart(ctypes.Structure):
+    _fields_ = [("csr_rowPtr_l", P), ("csr_colIdx_l", P), ("csr_rowIdx_zip_l", P), ("csr_val_l", P),
+                ("csc_colPtr_r", P), ("csc_rowIdx_r", P), ("csc_colIdx_zip_r", P), ("csc_val_r", P),
+                ("local_row_lb", I32), ("remote_col_lb", I32), ("local_row_num", I32), ("remote_col_num", I32)]
+
+
 class ServerOpts(ctypes.Structure):
     _fields_ = [("memory_budget", I64), ("slots", I32), ("max_group", I32), ("group_mib", I32),
                 ("small_mib", I32), ("copy_chunk_mib", I32), ("reserved", I32 * 1)]
@@ -124,6 +130,7 @@ SIGNATURES = {
     "cola_ppl0_batch_buffer_spmm_noalloc": (I32, [P, P] + [P] * 8 + [I32] * 7 + [P]),
     "cola_ppl_batch_spmm": (I32, [P, P, P, P, P, P] + [I32] * 5 + [P] + [I32] * 5 + [P]),
     "cola_zip_rows_create": (I32, [P] * 8 + [I32] * 6 + [P, P]),
+    "cola_zip_rows_create_all": (I32, [P, I32, I32, P, P]),
     "cola_zip_rows_spmm": (I32, [P, P, P, I32, P]),
     "cola_zip_rows_free": (I32, [P]),
     "cola_zip_rows_get_info": (I32, [P, P, P, P, P]),

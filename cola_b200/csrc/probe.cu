@@ -1,7 +1,8 @@
 // Ceilings of the row gather the SpMM kernels are made of, measured on the
 // device they run on (cola_probe_gather): warps read whole rows of a table
-// (16-byte vector loads across the warp, `unroll` rows in flight per warp, a
-// persistent grid of one full wave) at pseudo-random row indices.  With a table
+// (16-byte vector loads across the warp, 4 rows in flight per warp as in the
+// SpMM, a persistent grid of one full wave) at pseudo-random row indices read
+// from an index array, 32 at a time, as the SpMM reads its entries.  With a table
 // that fits in L2 the rows come from L2 (the ceiling of the SpMM's gathers,
 // most of which hit L2); with a table several times larger than L2 they come
 // from DRAM.  The sums are kept (one value per warp) so that no load is dead.
@@ -26,26 +27,38 @@ __device__ __forceinline__ uint32_t mix32(uint64_t x)
     return (uint32_t)x;
 }
 
+__global__ void make_indices_kernel(int32_t *__restrict__ idx, int64_t n, int64_t rows, uint64_t seed)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        idx[i] = (int32_t)(mix32(seed + (uint64_t)i) % (uint64_t)rows);
+}
+
+// The SpMM's gather loop without the arithmetic: a warp reads 32 row indices
+// with one coalesced load, then the rows they name, UNROLL rows in flight
+// (16-byte vectors across the warp).
 template <int UNROLL>
-__global__ void __launch_bounds__(256) gather_probe_kernel(const uint4 *__restrict__ table, int64_t rows,
-                                                           int row_vecs, int64_t gathers, uint64_t seed,
-                                                           float *__restrict__ sink)
+__global__ void __launch_bounds__(256) gather_probe_kernel(const uint4 *__restrict__ table, const int32_t *__restrict__ idx,
+                                                           int row_vecs, int64_t gathers, float *__restrict__ sink)
 {
     const int lane = threadIdx.x & 31;
     const int64_t warp = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
     const int64_t nwarps = (int64_t)gridDim.x * 8;
     uint32_t acc = 0;
-    for (int64_t g0 = warp * UNROLL; g0 < gathers; g0 += nwarps * UNROLL) {
-        uint4 v[UNROLL];
+    for (int64_t g0 = warp * 32; g0 < gathers; g0 += nwarps * 32) {
+        const int n = (int)min((int64_t)32, gathers - g0);
+        const int32_t mine = lane < n ? __ldcs(idx + g0 + lane) : 0;
+        for (int j = 0; j < n; j += UNROLL) {
+            uint4 v[UNROLL];
 #pragma unroll
-        for (int u = 0; u < UNROLL; u++) {
-            const int64_t r = (int64_t)(mix32(seed + (uint64_t)(g0 + u)) % (uint64_t)rows);
-            const uint4 *p = table + r * row_vecs;
-            v[u] = lane < row_vecs ? __ldg(p + lane) : make_uint4(0, 0, 0, 0);
+            for (int u = 0; u < UNROLL; u++) {
+                const int k = j + u;
+                const int32_t r = __shfl_sync(0xffffffffu, mine, k & 31);
+                v[u] = (k < n && lane < row_vecs) ? __ldg(table + (int64_t)r * row_vecs + lane) : make_uint4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < UNROLL; u++)
+                acc += v[u].x ^ v[u].y ^ v[u].z ^ v[u].w;
         }
-#pragma unroll
-        for (int u = 0; u < UNROLL; u++)
-            acc += v[u].x ^ v[u].y ^ v[u].z ^ v[u].w;
     }
     if (acc == 0x9e3779b9u)  // practically never: keeps the loads alive
         sink[warp] = (float)acc;
@@ -67,12 +80,19 @@ extern "C" cola_status cola_probe_gather(int64_t table_bytes, int32_t row_bytes,
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t rows = table_bytes / row_bytes;
     void *table = nullptr;
+    int32_t *idx = nullptr;
     float *sink = nullptr;
-    const int blocks = sm_count() * blocks_per_sm((const void *)probe::gather_probe_kernel<8>, 256);
+    const int blocks = sm_count() * blocks_per_sm((const void *)probe::gather_probe_kernel<4>, 256);
     COLA_CUDA(cudaMallocAsync(&table, (size_t)(rows * row_bytes), st));
     cudaError_t e = cudaMallocAsync((void **)&sink, (size_t)blocks * 8 * sizeof(float), st);
     if (e == cudaSuccess)
+        e = cudaMallocAsync((void **)&idx, (size_t)gathers * sizeof(int32_t), st);
+    if (e == cudaSuccess)
         e = cudaMemsetAsync(table, 0x5a, (size_t)(rows * row_bytes), st);
+    if (e == cudaSuccess) {
+        probe::make_indices_kernel<<<sm_count() * 8, 256, 0, st>>>(idx, gathers, rows, 0x1234567ull);
+        e = cudaGetLastError();
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (e == cudaSuccess)
         e = cudaEventCreate(&e0);
@@ -82,9 +102,8 @@ extern "C" cola_status cola_probe_gather(int64_t table_bytes, int32_t row_bytes,
     for (int pass = 0; pass < 2 && e == cudaSuccess; pass++) {  // pass 0 warms the cache
         e = cudaEventRecord(e0, st);
         for (int r = 0; r < (pass ? reps : 1) && e == cudaSuccess; r++) {
-            probe::gather_probe_kernel<8><<<blocks, 256, 0, st>>>(static_cast<const uint4 *>(table), rows,
-                                                                  row_bytes / 16, gathers, 0x1234567ull + 977ull * r,
-                                                                  sink);
+            probe::gather_probe_kernel<4><<<blocks, 256, 0, st>>>(static_cast<const uint4 *>(table), idx,
+                                                                  row_bytes / 16, gathers, sink);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess)
@@ -98,6 +117,7 @@ extern "C" cola_status cola_probe_gather(int64_t table_bytes, int32_t row_bytes,
         cudaEventDestroy(e0);
     if (e1)
         cudaEventDestroy(e1);
+    cudaFreeAsync(idx, st);
     cudaFreeAsync(sink, st);
     cudaFreeAsync(table, st);
     COLA_CUDA(e);

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <new>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -28,12 +29,13 @@ namespace zr {
 
 // Entries [e0, e0 + count) of a chunked block: chunk c (c0 <= c < c0 + nch)
 // covers [ptr[c], ptr[c+1]) and names target[c]; the entry's own index array
-// holds the other coordinate.  Local CSR chunks: row = target, column =
-// col_off + index.  Remote CSC chunks (remote = 1): column = target, row =
-// index.
+// holds the other coordinate.  Local CSR chunks: row = row_off + target,
+// column = col_off + index.  Remote CSC chunks (remote = 1): column = target,
+// row = row_off + index.
 __global__ void expand_chunks_kernel(const int32_t *__restrict__ ptr, const int32_t *__restrict__ target,
                                      const int32_t *__restrict__ index, const float *__restrict__ val, int64_t c0,
-                                     int64_t nch, int64_t e0, int64_t count, int64_t col_off, int remote,
+                                     int64_t nch, int64_t e0, int64_t count, int64_t col_off, int64_t row_off,
+                                     int remote,
                                      int32_t *__restrict__ out_row, int32_t *__restrict__ out_col,
                                      float *__restrict__ out_val, unsigned int *__restrict__ max_row,
                                      unsigned int *__restrict__ max_col, unsigned int *__restrict__ ok)
@@ -51,7 +53,7 @@ __global__ void expand_chunks_kernel(const int32_t *__restrict__ ptr, const int3
                 hi = m;
         }
         const int64_t t = __ldg(target + lo), x = __ldg(index + e);
-        const int64_t r = remote ? x : t;
+        const int64_t r = row_off + (remote ? x : t);
         const int64_t c = remote ? t : col_off + x;
         if (r < 0 || c < 0 || r > INT32_MAX || c > INT32_MAX) {
             atomicMin(ok, 0u);  // reported by the host
@@ -85,48 +87,52 @@ static cola_status read_i32(const int32_t *d, int64_t i, int32_t &v, cudaStream_
 
 using namespace cola;
 
-extern "C" {
+namespace cola {
+namespace zr {
 
-cola_status cola_zip_rows_create(const int32_t *csr_rowPtr_l, const int32_t *csr_colIdx_l,
-                                 const int32_t *csr_rowIdx_zip_l, const float *csr_val_l, const int32_t *csc_colPtr_r,
-                                 const int32_t *csc_rowIdx_r, const int32_t *csc_colIdx_zip_r, const float *csc_val_r,
-                                 int32_t local_row_lb, int32_t remote_col_lb, int32_t local_row_num,
-                                 int32_t remote_col_num, int32_t nodesPerPE, int32_t peid, cola_stream_t stream,
-                                 cola_zip_rows **out)
+// The row view of the chunks of several PEs' calls: PE part[i] (whose rows
+// start at output row row0[i]) contributes its local chunks [llb, +lnum) and
+// remote chunks [rlb, +rnum).  x_peid: the PE whose X slice the SpMM calls
+// will pass as `input`.
+static cola_status build(const cola_zip_part *parts, int32_t nparts, const int64_t *row0, int32_t nodesPerPE,
+                         const int32_t *peids, int32_t x_peid, cudaStream_t st, cola_zip_rows **out, const char *who)
 {
-    const char *who = "cola_zip_rows_create";
-    COLA_REQUIRE(out, COLA_ERROR_INVALID_ARGUMENT, "%s: out is NULL", who);
-    *out = nullptr;
-    clear_error();
-    COLA_REQUIRE(local_row_lb >= 0 && remote_col_lb >= 0 && local_row_num >= 0 && remote_col_num >= 0 &&
-                     nodesPerPE >= 1 && peid >= 0,
-                 COLA_ERROR_INVALID_ARGUMENT, "%s: negative chunk range, nodesPerPE %d or peid %d", who, nodesPerPE,
-                 peid);
-    COLA_REQUIRE(local_row_num == 0 || (csr_rowPtr_l && csr_colIdx_l && csr_rowIdx_zip_l), COLA_ERROR_INVALID_ARGUMENT,
-                 "%s: null local CSR arrays", who);
-    COLA_REQUIRE(remote_col_num == 0 || (csc_colPtr_r && csc_rowIdx_r && csc_colIdx_zip_r),
-                 COLA_ERROR_INVALID_ARGUMENT, "%s: null remote CSC arrays", who);
-    cudaStream_t st = (cudaStream_t)stream;
-    // entry ranges of the chunks the call covers (chunk pointers are monotonic)
-    int32_t lb_e = 0, le_e = 0, rb_e = 0, re_e = 0;
-    if (local_row_num > 0) {
-        COLA_TRY(zr::read_i32(csr_rowPtr_l, local_row_lb, lb_e, st));
-        COLA_TRY(zr::read_i32(csr_rowPtr_l, (int64_t)local_row_lb + local_row_num, le_e, st));
-    }
-    if (remote_col_num > 0) {
-        COLA_TRY(zr::read_i32(csc_colPtr_r, remote_col_lb, rb_e, st));
-        COLA_TRY(zr::read_i32(csc_colPtr_r, (int64_t)remote_col_lb + remote_col_num, re_e, st));
+    std::vector<int32_t> ends((size_t)nparts * 4, 0);
+    for (int32_t i = 0; i < nparts; i++) {
+        const cola_zip_part &z = parts[i];
+        COLA_REQUIRE(z.local_row_lb >= 0 && z.remote_col_lb >= 0 && z.local_row_num >= 0 && z.remote_col_num >= 0,
+                     COLA_ERROR_INVALID_ARGUMENT, "%s: PE %d: negative chunk range", who, i);
+        COLA_REQUIRE(z.local_row_num == 0 || (z.csr_rowPtr_l && z.csr_colIdx_l && z.csr_rowIdx_zip_l),
+                     COLA_ERROR_INVALID_ARGUMENT, "%s: PE %d: null local CSR arrays", who, i);
+        COLA_REQUIRE(z.remote_col_num == 0 || (z.csc_colPtr_r && z.csc_rowIdx_r && z.csc_colIdx_zip_r),
+                     COLA_ERROR_INVALID_ARGUMENT, "%s: PE %d: null remote CSC arrays", who, i);
+        // entry ranges of the chunks the call covers (chunk pointers are monotonic)
+        if (z.local_row_num > 0) {
+            COLA_TRY(read_i32(z.csr_rowPtr_l, z.local_row_lb, ends[(size_t)i * 4], st));
+            COLA_TRY(read_i32(z.csr_rowPtr_l, (int64_t)z.local_row_lb + z.local_row_num, ends[(size_t)i * 4 + 1], st));
+        }
+        if (z.remote_col_num > 0) {
+            COLA_TRY(read_i32(z.csc_colPtr_r, z.remote_col_lb, ends[(size_t)i * 4 + 2], st));
+            COLA_TRY(read_i32(z.csc_colPtr_r, (int64_t)z.remote_col_lb + z.remote_col_num, ends[(size_t)i * 4 + 3],
+                              st));
+        }
     }
     COLA_CUDA(cudaStreamSynchronize(st));
-    COLA_REQUIRE(le_e >= lb_e && re_e >= rb_e, COLA_ERROR_INVALID_ARGUMENT, "%s: chunk pointers decrease", who);
-    const int64_t nl = (int64_t)le_e - lb_e, nr = (int64_t)re_e - rb_e, nnz = nl + nr;
+    int64_t nnz = 0;
+    for (int32_t i = 0; i < nparts; i++) {
+        const int32_t *e = ends.data() + (size_t)i * 4;
+        COLA_REQUIRE(e[1] >= e[0] && e[3] >= e[2], COLA_ERROR_INVALID_ARGUMENT, "%s: PE %d: chunk pointers decrease",
+                     who, i);
+        nnz += (int64_t)(e[1] - e[0]) + (e[3] - e[2]);
+    }
+    COLA_REQUIRE(nnz < (int64_t)INT32_MAX, COLA_ERROR_UNSUPPORTED, "%s: %lld entries (at most 2^31 - 1)", who,
+                 (long long)nnz);
 
     void *arena = nullptr;
     const size_t a = 256, n = (size_t)std::max<int64_t>(nnz, 1);
-    const size_t bytes = 3 * ((4 * n + a - 1) / a * a) + a;
-    COLA_CUDA(cudaMallocAsync(&arena, bytes, st));
-    char *base = static_cast<char *>(arena);
     const size_t slice = (4 * n + a - 1) / a * a;
+    COLA_CUDA(cudaMallocAsync(&arena, 3 * slice + a, st));
+    char *base = static_cast<char *>(arena);
     int32_t *row = reinterpret_cast<int32_t *>(base);
     int32_t *col = reinterpret_cast<int32_t *>(base + slice);
     float *val = reinterpret_cast<float *>(base + 2 * slice);
@@ -136,17 +142,26 @@ cola_status cola_zip_rows_create(const int32_t *csr_rowPtr_l, const int32_t *csr
     {
         const unsigned int init[3] = {0u, 0u, 1u};
         cudaError_t e = cudaMemcpyAsync(mx, init, sizeof init, cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess && nl > 0) {
-            zr::expand_chunks_kernel<<<zr::blocks_for(nl), 256, 0, st>>>(
-                csr_rowPtr_l, csr_rowIdx_zip_l, csr_colIdx_l, csr_val_l, local_row_lb, local_row_num, lb_e, nl,
-                (int64_t)peid * nodesPerPE, 0, row, col, val, mx, mx + 1, mx + 2);
-            e = cudaGetLastError();
-        }
-        if (e == cudaSuccess && nr > 0) {
-            zr::expand_chunks_kernel<<<zr::blocks_for(nr), 256, 0, st>>>(
-                csc_colPtr_r, csc_colIdx_zip_r, csc_rowIdx_r, csc_val_r, remote_col_lb, remote_col_num, rb_e, nr, 0,
-                1, row + nl, col + nl, val + nl, mx, mx + 1, mx + 2);
-            e = cudaGetLastError();
+        int64_t at = 0;
+        for (int32_t i = 0; i < nparts && e == cudaSuccess; i++) {
+            const cola_zip_part &z = parts[i];
+            const int32_t *en = ends.data() + (size_t)i * 4;
+            const int64_t nl = (int64_t)en[1] - en[0], nr = (int64_t)en[3] - en[2];
+            if (nl > 0) {
+                expand_chunks_kernel<<<blocks_for(nl), 256, 0, st>>>(
+                    z.csr_rowPtr_l, z.csr_rowIdx_zip_l, z.csr_colIdx_l, z.csr_val_l, z.local_row_lb, z.local_row_num,
+                    en[0], nl, (int64_t)peids[i] * nodesPerPE, row0[i], 0, row + at, col + at, val + at, mx, mx + 1,
+                    mx + 2);
+                e = cudaGetLastError();
+                at += nl;
+            }
+            if (e == cudaSuccess && nr > 0) {
+                expand_chunks_kernel<<<blocks_for(nr), 256, 0, st>>>(
+                    z.csc_colPtr_r, z.csc_colIdx_zip_r, z.csc_rowIdx_r, z.csc_val_r, z.remote_col_lb,
+                    z.remote_col_num, en[2], nr, 0, row0[i], 1, row + at, col + at, val + at, mx, mx + 1, mx + 2);
+                e = cudaGetLastError();
+                at += nr;
+            }
         }
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(h_mx, mx, sizeof h_mx, cudaMemcpyDeviceToHost, st);
@@ -175,10 +190,53 @@ cola_status cola_zip_rows_create(const int32_t *csr_rowPtr_l, const int32_t *csr
     }
     h->g = g;
     h->npp = nodesPerPE;
-    h->peid = peid;
+    h->peid = x_peid;
     h->nnz = nnz;
     *out = h;
     return COLA_SUCCESS;
+}
+
+}  // namespace zr
+}  // namespace cola
+
+extern "C" {
+
+cola_status cola_zip_rows_create(const int32_t *csr_rowPtr_l, const int32_t *csr_colIdx_l,
+                                 const int32_t *csr_rowIdx_zip_l, const float *csr_val_l, const int32_t *csc_colPtr_r,
+                                 const int32_t *csc_rowIdx_r, const int32_t *csc_colIdx_zip_r, const float *csc_val_r,
+                                 int32_t local_row_lb, int32_t remote_col_lb, int32_t local_row_num,
+                                 int32_t remote_col_num, int32_t nodesPerPE, int32_t peid, cola_stream_t stream,
+                                 cola_zip_rows **out)
+{
+    const char *who = "cola_zip_rows_create";
+    COLA_REQUIRE(out, COLA_ERROR_INVALID_ARGUMENT, "%s: out is NULL", who);
+    *out = nullptr;
+    clear_error();
+    COLA_REQUIRE(nodesPerPE >= 1 && peid >= 0, COLA_ERROR_INVALID_ARGUMENT, "%s: nodesPerPE %d, peid %d", who,
+                 nodesPerPE, peid);
+    const cola_zip_part z = {csr_rowPtr_l,  csr_colIdx_l, csr_rowIdx_zip_l, csr_val_l,     csc_colPtr_r,
+                             csc_rowIdx_r,  csc_colIdx_zip_r, csc_val_r,    local_row_lb,  remote_col_lb,
+                             local_row_num, remote_col_num};
+    const int64_t row0 = 0;
+    return zr::build(&z, 1, &row0, nodesPerPE, &peid, peid, (cudaStream_t)stream, out, who);
+}
+
+cola_status cola_zip_rows_create_all(const cola_zip_part *parts, int32_t nparts, int32_t nodesPerPE,
+                                     cola_stream_t stream, cola_zip_rows **out)
+{
+    const char *who = "cola_zip_rows_create_all";
+    COLA_REQUIRE(out, COLA_ERROR_INVALID_ARGUMENT, "%s: out is NULL", who);
+    *out = nullptr;
+    clear_error();
+    COLA_REQUIRE(parts && nparts >= 1 && nodesPerPE >= 1, COLA_ERROR_INVALID_ARGUMENT,
+                 "%s: %d PEs, nodesPerPE %d", who, nparts, nodesPerPE);
+    std::vector<int64_t> row0((size_t)nparts);
+    std::vector<int32_t> peids((size_t)nparts);
+    for (int32_t i = 0; i < nparts; i++) {
+        row0[(size_t)i] = (int64_t)i * nodesPerPE;
+        peids[(size_t)i] = i;
+    }
+    return zr::build(parts, nparts, row0.data(), nodesPerPE, peids.data(), 0, (cudaStream_t)stream, out, who);
 }
 
 cola_status cola_zip_rows_spmm(cola_zip_rows *h, float *output, const float *input, int32_t dim,

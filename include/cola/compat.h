@@ -24,7 +24,9 @@
  *    destroyed; every call then runs the row-major schedule on it (one writer
  *    per row, no atomics, the same bits every call) instead of the chunk
  *    kernel.  The result is the same product; arrays not owned by a holder
- *    run the chunk kernel.  cola_compat::set_row_view_cache(false) turns the
+ *    run the chunk kernel.  distSpMM_ppl_batch_all with a single stage does
+ *    the same with one row view of every PE's chunks: one launch (plus one for
+ *    hub rows) for all PEs.  cola_compat::set_row_view_cache(false) turns the
  *    cache off.
  */
 #ifndef COLA_COMPAT_H
@@ -84,6 +86,8 @@ struct zip_registry {
     std::mutex mu;
     std::map<const void *, arrays> csr, csc;  // holder -> its four device arrays
     std::map<view_key, cola_zip_rows *> views;
+    // all PEs at once: nparts, nodesPerPE, then per PE its two holders and four offsets
+    std::map<std::vector<intptr_t>, cola_zip_rows *> all_views;
     bool enabled = true;
 };
 
@@ -119,6 +123,63 @@ inline void forget_holder(bool is_csr, const void *holder)
             ++it;
         }
     }
+    for (auto it = R.all_views.begin(); it != R.all_views.end();) {
+        bool uses = false;
+        for (size_t i = 2; i < it->first.size(); i += 6)
+            uses = uses || it->first[i + (is_csr ? 0 : 1)] == (intptr_t)holder;
+        if (uses) {
+            cola_zip_rows_free(it->second);
+            it = R.all_views.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
+// The row view of every PE's single-stage call at once (PE p's holders and
+// chunk ranges), built on first use, when every block belongs to a holder.
+inline cola_zip_rows *cached_all_view(int nranks, int nodesPerPE, void *const *csr_holders,
+                                      void *const *csc_holders, int *const *local_offset, int *const *remote_offset,
+                                      cudaStream_t stream)
+{
+    zip_registry &R = registry();
+    std::lock_guard<std::mutex> lk(R.mu);
+    if (!R.enabled)
+        return nullptr;
+    std::vector<intptr_t> key{(intptr_t)nranks, (intptr_t)nodesPerPE};
+    for (int p = 0; p < nranks; p++) {
+        if (!R.csr.count(csr_holders[p]) || !R.csc.count(csc_holders[p]))
+            return nullptr;
+        key.insert(key.end(), {(intptr_t)csr_holders[p], (intptr_t)csc_holders[p], (intptr_t)local_offset[p][0],
+                               (intptr_t)remote_offset[p][0], (intptr_t)(local_offset[p][1] - local_offset[p][0]),
+                               (intptr_t)(remote_offset[p][1] - remote_offset[p][0])});
+    }
+    auto it = R.all_views.find(key);
+    if (it != R.all_views.end())
+        return it->second;
+    std::vector<cola_zip_part> parts((size_t)nranks);
+    for (int p = 0; p < nranks; p++) {
+        const auto &l = R.csr[csr_holders[p]];
+        const auto &r = R.csc[csc_holders[p]];
+        cola_zip_part &z = parts[(size_t)p];
+        z.csr_rowPtr_l = static_cast<const int32_t *>(std::get<0>(l));
+        z.csr_colIdx_l = static_cast<const int32_t *>(std::get<1>(l));
+        z.csr_rowIdx_zip_l = static_cast<const int32_t *>(std::get<2>(l));
+        z.csr_val_l = static_cast<const float *>(std::get<3>(l));
+        z.csc_colPtr_r = static_cast<const int32_t *>(std::get<0>(r));
+        z.csc_rowIdx_r = static_cast<const int32_t *>(std::get<1>(r));
+        z.csc_colIdx_zip_r = static_cast<const int32_t *>(std::get<2>(r));
+        z.csc_val_r = static_cast<const float *>(std::get<3>(r));
+        z.local_row_lb = local_offset[p][0];
+        z.remote_col_lb = remote_offset[p][0];
+        z.local_row_num = local_offset[p][1] - local_offset[p][0];
+        z.remote_col_num = remote_offset[p][1] - remote_offset[p][0];
+    }
+    cola_zip_rows *h = nullptr;
+    check(cola_zip_rows_create_all(parts.data(), nranks, nodesPerPE, (cola_stream_t)stream, &h),
+          "distSpMM_ppl_batch_all (row view)");
+    R.all_views[key] = h;
+    return h;
 }
 
 // The row view for these arrays and chunk range when both blocks belong to
@@ -391,6 +452,20 @@ inline void distSpMM_ppl_batch_all(const int group_size, float *output, const fl
 {
     const int nstages = nranks / group_size;
     const long long pe = (long long)nodesPerPE * dim;
+    if (nstages == 1) {
+        // one stage: every PE's chunks in one row view, one launch for all of them
+        std::vector<void *> hl((size_t)nranks), hr((size_t)nranks);
+        for (int me = 0; me < nranks; me++) {
+            hl[(size_t)me] = csr_zip_l[me];
+            hr[(size_t)me] = csc_zip_r[me];
+        }
+        if (cola_zip_rows *h = cola_compat::cached_all_view(nranks, nodesPerPE, hl.data(), hr.data(),
+                                                             local_offset_ppl, remote_offset_ppl, stream)) {
+            cola_compat::check(cola_zip_rows_spmm(h, output, input_nvsh, dim, (cola_stream_t)stream),
+                               "distSpMM_ppl_batch_all");
+            return;
+        }
+    }
     for (int me = 0; me < nranks; me++)
         ppl0_batch_SpMM<1, false>(output + me * pe, input_nvsh + me * pe, csr_zip_l[me]->d_csr_rowPtr,
                                   csr_zip_l[me]->d_csr_colIdx, csr_zip_l[me]->d_csr_rowIdx_zip,

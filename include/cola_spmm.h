@@ -276,6 +276,22 @@ cola_status cola_zip_rows_create(const int32_t *csr_rowPtr_l, const int32_t *csr
                                  int32_t local_row_lb, int32_t remote_col_lb, int32_t local_row_num,
                                  int32_t remote_col_num, int32_t nodesPerPE, int32_t peid, cola_stream_t stream,
                                  cola_zip_rows **out);
+/* One PE's arguments for cola_zip_rows_create_all: its zip arrays and the
+ * chunk ranges its ppl0_batch_SpMM call covers. */
+typedef struct cola_zip_part {
+    const int32_t *csr_rowPtr_l, *csr_colIdx_l, *csr_rowIdx_zip_l;
+    const float *csr_val_l;
+    const int32_t *csc_colPtr_r, *csc_rowIdx_r, *csc_colIdx_zip_r;
+    const float *csc_val_r;
+    int32_t local_row_lb, remote_col_lb, local_row_num, remote_col_num;
+} cola_zip_part;
+/* The row view of every PE's call at once (PE p = parts[p], its output rows
+ * starting at row p*nodesPerPE of the symmetric output): one
+ * cola_zip_rows_spmm(h, output, input, dim) with output and input at PE 0's
+ * slices then adds what the nparts per-PE calls add, in one launch (plus one
+ * for hub rows) instead of one per PE. */
+cola_status cola_zip_rows_create_all(const cola_zip_part *parts, int32_t nparts, int32_t nodesPerPE,
+                                     cola_stream_t stream, cola_zip_rows **out);
 /* output[r] += sum of the covered entries of row r times input rows (input =
  * PE peid's slice of the symmetric X, as for cola_ppl0_batch_spmm); FP32,
  * any dim >= 1.  Asynchronous on `stream`. */
@@ -368,7 +384,7 @@ cola_status cola_set_gather_wait_limit(int64_t polls);
 
 /* The row-gather ceiling of the current device: warps read whole rows of
  * row_bytes (16..512) from a table of table_bytes at pseudo-random row indices
- * (16-byte loads, 8 rows in flight per warp, one full wave), `gathers` rows per
+ * (16-byte loads, 4 rows in flight per warp, one full wave), `gathers` rows per
  * run, `reps` timed runs after one warm-up run; *gbps = row bytes read per
  * second.  A table that fits in L2 measures the L2 ceiling of the SpMM's
  * gathers, a table far larger than L2 the DRAM ceiling.  Allocates the table

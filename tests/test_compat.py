@@ -44,7 +44,9 @@ def test_compat_reference_main_on_gpu(tmp_path, P, dim):
     """A host program written like the reference's main (bin2vec the partition
     files, nnz_split both blocks, d_csr_zip / d_csc_zip, run_distSpMM_ppl_batch
     with validation against SAG_reference_host and a timed loop), built against
-    compat.h, passes its own validation on the GPU for every virtual PE."""
+    compat.h, passes its own validation on the GPU for every virtual PE; and
+    the same holders in one distSpMM_ppl_batch_all call (single stage: one row
+    view of all PEs) give the same product."""
     import scipy.sparse as sp
     exe = str(tmp_path / "compat_gpu_main")
     cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
@@ -64,3 +66,6 @@ def test_compat_reference_main_on_gpu(tmp_path, P, dim):
     for p in range(P):
         assert "PEid-{} passed".format(p) in out
         assert any(l.startswith("PE {} ms ".format(p)) and float(l.split()[-1]) > 0 for l in out)
+    # distSpMM_ppl_batch_all, single stage: one row view of every PE's chunks
+    rel_all = [float(l.split()[-1]) for l in out if l.startswith("ALL rel ")]
+    assert rel_all and rel_all[0] <= 1e-5

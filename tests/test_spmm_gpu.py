@@ -595,3 +595,46 @@ def test_zip_rows_view_matches_reference_kernels_and_rows(K):
     if oracle.ref_available():
         theirs = _run_reference(g, Xd, npp, K, P)[:n].cpu().numpy()
         assert rel(y.cpu().numpy(), theirs) <= TOL_F32
+
+
+@pytest.mark.parametrize("K", [32, 128])
+def test_zip_rows_all_pes_one_view(K):
+    """Every PE's chunks in one row view (cola_zip_rows_create_all, what
+    compat.h's single-stage distSpMM_ppl_batch_all keeps): one call adds the
+    whole product, equal to the graph's own row-major output (bit for bit
+    where one lane group takes a row), within 1e-5 of FP64."""
+    P = 4
+    n, row, col, val, ps = graph_case(12, 16, seed=23, nparts=P)
+    g = S.Graph(ps)
+    npp = g.nodes_per_part
+    X = _padded_x(n, P, npp, K, seed=K)
+    Xd = torch.from_numpy(X).to(DEV)
+    parts = (cb._lib.ZipPart * P)()
+    for p in range(P):
+        z = g.zip_view(p)
+        q = parts[p]
+        q.csr_rowPtr_l, q.csr_colIdx_l, q.csr_rowIdx_zip_l, q.csr_val_l = (z.csr_rowPtr, z.csr_colIdx,
+                                                                           z.csr_rowIdx_zip, z.csr_val)
+        q.csc_colPtr_r, q.csc_rowIdx_r, q.csc_colIdx_zip_r, q.csc_val_r = (z.csc_colPtr, z.csc_rowIdx,
+                                                                           z.csc_colIdx_zip, z.csc_val)
+        q.local_row_lb, q.remote_col_lb, q.local_row_num, q.remote_col_num = 0, 0, z.local_chunks, z.remote_chunks
+    L = cb.lib()
+    h = ctypes.c_void_p()
+    cb._lib.check(L.cola_zip_rows_create_all(parts, P, npp, None, ctypes.byref(h)))
+    try:
+        Y = torch.zeros((P * npp, K), device=DEV)
+        cb._lib.check(L.cola_zip_rows_spmm(h, ptr(Y), ptr(Xd), K, None))
+        torch.cuda.synchronize()
+        nnz = ctypes.c_int64()
+        cb._lib.check(L.cola_zip_rows_get_info(h, None, ctypes.byref(nnz), None, None))
+        assert nnz.value == g.info.nnz
+    finally:
+        L.cola_zip_rows_free(h)
+    rows = g.spmm(Xd[:n], schedule=S.SCHEDULE_ROWS)
+    y = Y[:n]
+    assert rel(y.cpu().numpy(), fp64_reference(n, row, col, val, X[:n])) <= TOL_F32
+    if K // 4 > 16:
+        assert torch.equal(y, rows)
+    else:
+        assert rel(y.cpu().numpy(), rows.cpu().numpy()) <= 1e-6
+    assert torch.all(Y[n:] == 0)
