@@ -140,6 +140,9 @@ SIGNATURES = {
     "cola_graph_get_info": (I32, [P, P]),
     "cola_graph_zip_view": (I32, [P, I32, P]),
     "cola_spmm": (I32, [P, P, I32, I64, P, I32, I64, I32, P, P]),
+    "cola_spmm_host": (I32, [P, P, I32, I64, P, I32, I64, I32, P, P]),
+    "cola_spmm_host_sync": (I32, [P]),
+    "cola_spmm_host_join": (I32, [P, P]),
     "cola_spmm_autotune": (I32, [P, P, I32, I64, P, I32, I64, I32, I32, I32, ctypes.c_char_p, P, P, P, P]),
     "cola_batch_create": (I32, [P, I32, P, P, P]),
     "cola_batch_create_from_graphs": (I32, [P, I32, P]),

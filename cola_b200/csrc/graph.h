@@ -39,6 +39,11 @@ cola_status ensure(void *&p, size_t &have, size_t need);
 using cola::dev::GatherSeg;
 using cola::dev::PartDesc;
 
+namespace cola {
+struct HostPipe;  // cola_spmm_host's staging sets and copy streams
+void host_pipe_release(HostPipe *p);
+}  // namespace cola
+
 struct cola_graph {
     int device = 0;
     int32_t N = 0, P = 0, npp = 0, gs = 0, nstages = 1, if_split = 1;
@@ -87,6 +92,7 @@ struct cola_graph {
     int32_t hub_threshold = 256, hub_segment = 256, task_entries = 256;
     float *ws_hub = nullptr;  // nseg x K partials
     size_t ws_hub_bytes = 0;
+    cola::HostPipe *host_pipe = nullptr;  // created by the first cola_spmm_host call
 };
 
 namespace cola {

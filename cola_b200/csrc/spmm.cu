@@ -722,6 +722,7 @@ void graph_release(cola_graph *g)
     cudaFree(g->stage_buf);
     cudaFree(g->ws);
     cudaFree(g->ws_hub);
+    host_pipe_release(g->host_pipe);
     cudaSetDevice(cur);
     delete g;
 }

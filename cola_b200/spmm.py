@@ -125,6 +125,31 @@ class Graph:
                               ctypes.byref(o), _stream(stream)))
         return Y
 
+    def spmm_host(self, X, Y, schedule=SCHEDULE_AUTO, stream=None):
+        """cola_spmm_host: Y = A X with X and Y host tensors (pinned for
+        overlap); returns at once, the result is in Y after sync_host()."""
+        for t, name in ((X, "X"), (Y, "Y")):
+            if not isinstance(t, torch.Tensor) or t.is_cuda or t.dim() != 2 or t.stride(1) != 1:
+                raise ValueError("{} must be a 2-D row-major host tensor".format(name))
+            if t.dtype not in _DT:
+                raise TypeError("{} must be float32 or bfloat16".format(name))
+        K = X.shape[1]
+        if X.shape[0] < self.num_nodes or Y.shape[0] < self.num_nodes or Y.shape[1] != K:
+            raise ValueError("X must have >= N rows and Y must be N x K")
+        o = SpmmOpts()
+        o.schedule = int(schedule)
+        check(lib().cola_spmm_host(self._h, _ptr(X), _DT[X.dtype], X.stride(0), _ptr(Y), _DT[Y.dtype], Y.stride(0),
+                                   K, ctypes.byref(o), _stream(stream)))
+        return Y
+
+    def sync_host(self):
+        """Wait for every spmm_host call made on this graph."""
+        check(lib().cola_spmm_host_sync(self._h))
+
+    def join_host(self, stream=None):
+        """Make `stream` wait for every spmm_host call made so far."""
+        check(lib().cola_spmm_host_join(self._h, _stream(stream)))
+
     def autotune(self, X, Y=None, out_dtype=None, schedule=SCHEDULE_AUTO, reps=5, cache_path=None, stream=None):
         """cola_spmm_autotune on these operands: returns (options dict for
         spmm(), best ms, whether it came from the cache file)."""

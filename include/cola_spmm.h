@@ -463,6 +463,24 @@ cola_status cola_spmm_autotune(cola_graph *g, const void *X, cola_dtype x_dtype,
                                const char *cache_path, cola_stream_t stream, cola_spmm_opts *best, float *best_ms,
                                int32_t *from_cache);
 
+/* Y = A X with X and Y in host memory (pinned memory lets the copies run
+ * asynchronously): X is copied in, multiplied as cola_spmm does (opts as
+ * there; accumulate is not supported) and Y copied out, asynchronously.  The
+ * graph keeps two device staging sets and two copy streams of its own, so
+ * consecutive calls overlap: call i + 1's upload runs while call i's result
+ * downloads, and the SpMMs run on `stream`.  X_host must hold the features
+ * when the call is made and stay unchanged, and Y_host untouched, until the
+ * call's work is complete: cola_spmm_host_sync(g) waits for every call made
+ * on the graph so far.  The staging sets (N x K elements of each dtype, twice)
+ * are allocated by the first calls and kept with the graph. */
+cola_status cola_spmm_host(cola_graph *g, const void *X_host, cola_dtype x_dtype, int64_t ldx, void *Y_host,
+                           cola_dtype y_dtype, int64_t ldy, int32_t K, const cola_spmm_opts *opts,
+                           cola_stream_t stream);
+cola_status cola_spmm_host_sync(cola_graph *g);
+/* Makes `stream` wait (without blocking the host) for every cola_spmm_host
+ * call made on the graph so far, Y downloads included. */
+cola_status cola_spmm_host_join(cola_graph *g, cola_stream_t stream);
+
 /* ========================================================================
  * Batched form: many graphs of uneven size, each with its own X, Y and
  * feature width, in one persistent launch (plus one for hub rows).

@@ -638,3 +638,34 @@ def test_zip_rows_all_pes_one_view(K):
     else:
         assert rel(y.cpu().numpy(), rows.cpu().numpy()) <= 1e-6
     assert torch.all(Y[n:] == 0)
+
+
+@pytest.mark.parametrize("xdt,ydt", [(torch.float32, torch.float32), (torch.bfloat16, torch.bfloat16)])
+def test_spmm_host_pipelined_calls(case12, xdt, ydt):
+    """cola_spmm_host: host X in, SpMM, host Y out, consecutive calls
+    overlapped by the library (two staging sets); every call's Y equals the
+    device call's bits, strided host rows included, and accumulate is
+    refused."""
+    n, row, col, val, ps = case12
+    g = S.Graph(ps)
+    K = 128
+    xs = [torch.from_numpy(dense_x(n, K, seed=s)).to(xdt).pin_memory() for s in (1, 2, 3)]
+    ys = [torch.empty((n, K), dtype=ydt).pin_memory() for _ in range(3)]
+    for x, y in zip(xs, ys):
+        g.spmm_host(x, y)
+    g.sync_host()
+    for x, y in zip(xs, ys):
+        want = g.spmm(x.to(DEV), out_dtype=ydt).cpu()
+        assert torch.equal(y, want)
+    # strided host rows: a view of wider matrices
+    xw = torch.zeros((n, K + 8), dtype=xdt).pin_memory()
+    xw[:, :K] = xs[0]
+    yw = torch.full((n, K + 4), 7.0, dtype=ydt).pin_memory()
+    g.spmm_host(xw[:, :K], yw[:, :K])
+    g.sync_host()
+    assert torch.equal(yw[:, :K], ys[0]) and torch.all(yw[:, K:] == 7.0)
+    o = cb._lib.SpmmOpts()
+    o.accumulate = 1
+    rc = cb.lib().cola_spmm_host(g._h, ptr(xs[0]), 0 if xdt == torch.float32 else 1, K, ptr(ys[0]),
+                                 0 if ydt == torch.float32 else 1, K, K, ctypes.byref(o), None)
+    assert rc == 4  # COLA_ERROR_UNSUPPORTED
