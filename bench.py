@@ -1086,7 +1086,7 @@ def serving_leg(args, seconds):
     t0 = time.time()
     rng = np.random.Generator(np.random.Philox(5))
     srv = Server(memory_budget=120 << 30, slots=4, max_group=16, small_mib=args.serve_small_mib,
-                 copy_chunk_mib=args.serve_chunk_mib)
+                 copy_chunk_mib=args.serve_chunk_mib, copy_engines_only=args.serve_copy_engines_only)
     gn, gnnz = [], []
     for i in range(args.serve_graphs):
         scale = int(rng.integers(12, 21))
@@ -1196,6 +1196,8 @@ def serving_leg(args, seconds):
             "peak_device_bytes": st["peak_bytes"], "budget_bytes": st["budget"],
             "per_size_class": per_class, "open_loop_seconds": round(wall, 2),
             "small_mib": args.serve_small_mib or 16, "copy_chunk_mib": args.serve_chunk_mib or 32,
+            "small_groups_copied_by": "copy engines" if args.serve_copy_engines_only else
+            "SM kernels on the pinned host buffers",
             "served_GBps": B / wall / 1e9, "prep_seconds": round(t_prep, 1),
             "latency": "submit to result in pinned host memory"}, B, wall, nreq, h2d, clk
 
@@ -1421,6 +1423,8 @@ def main():
     ap.add_argument("--serve-small-mib", type=int, default=0,
                     help="serving: size-class threshold in MiB of copies (0 = library default 16, -1 = FIFO)")
     ap.add_argument("--serve-chunk-mib", type=int, default=0, help="serving: copy piece size (0 = library default)")
+    ap.add_argument("--serve-copy-engines-only", action="store_true",
+                    help="serving: small groups copy with the copy engines too (no SM copies)")
     ap.add_argument("--batch-graphs", type=int, default=512, help="batched workload: number of graphs")
     ap.add_argument("--tune-cache", default=None, help="batched workload: autotuner cache file (tuned once per shape)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "buffer", "rows"])

@@ -83,7 +83,7 @@ class ZipPart(ctypes.Structure):
 
 class ServerOpts(ctypes.Structure):
     _fields_ = [("memory_budget", I64), ("slots", I32), ("max_group", I32), ("group_mib", I32),
-                ("small_mib", I32), ("copy_chunk_mib", I32), ("reserved", I32 * 1)]
+                ("small_mib", I32), ("copy_chunk_mib", I32), ("copy_engines_only", I32)]
 
 
 class ServerStats(ctypes.Structure):

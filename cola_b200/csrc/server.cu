@@ -77,6 +77,7 @@ struct cola_server {
     int64_t small_bytes = 16 << 20;  // size classes (server_policy.h); 0 = off
     int32_t small_slots = 1;
     int64_t copy_chunk = 32 << 20;
+    bool sm_copies = true;  // small groups copy with the SMs (copy_by_sms_kernel)
     std::vector<cola_graph *> graphs;
     std::vector<Slot> slots;
     // request buffers come from a pool of the server's own that keeps freed
@@ -122,6 +123,56 @@ static cola_status copy_chunked(void *dst, const void *src, size_t bytes, cudaMe
     return COLA_SUCCESS;
 }
 
+// Copies by the SMs instead of the copy engines, for small groups: the copy
+// engines take copies in the order they were queued, so a small request's
+// copy queued behind another slot's gigabyte would wait for all of it.  Pinned
+// host memory is addressable from the device (unified addressing), so a
+// kernel moves the bytes itself; writes to host memory are fenced system-wide
+// before the kernel ends.  n16: 16-byte units; both pointers 16-byte aligned.
+__global__ void __launch_bounds__(256) copy_by_sms_kernel(uint4 *__restrict__ dst, const uint4 *__restrict__ src,
+                                                           int64_t n16, int to_host)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n16; i += 4 * stride) {  // four loads in flight per thread
+        const uint4 a = src[i], b = src[i + stride], c = src[i + 2 * stride], d = src[i + 3 * stride];
+        dst[i] = a;
+        dst[i + stride] = b;
+        dst[i + 2 * stride] = c;
+        dst[i + 3 * stride] = d;
+    }
+    for (; i < n16; i += stride)
+        dst[i] = src[i];
+    if (to_host)
+        __threadfence_system();
+}
+
+// Whether the SMs can copy `bytes` between these pointers: the host side
+// pinned and addressable from the device, both 16-byte aligned.
+static bool sm_copy_ok(const void *host, const void *dev, size_t bytes)
+{
+    if (((uintptr_t)host | (uintptr_t)dev | bytes) & 15u)
+        return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, host) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost && at.devicePointer == host;
+}
+
+static cola_status copy_by_sms(void *dst, const void *src, size_t bytes, bool to_host, cudaStream_t st)
+{
+    const int64_t n16 = (int64_t)(bytes / 16);
+    if (n16 == 0)
+        return COLA_SUCCESS;
+    const int blocks = (int)std::min<int64_t>((n16 + 1023) / 1024, 128);
+    copy_by_sms_kernel<<<blocks, 256, 0, st>>>(static_cast<uint4 *>(dst), static_cast<const uint4 *>(src), n16,
+                                               to_host ? 1 : 0);
+    COLA_CUDA(cudaGetLastError());
+    return COLA_SUCCESS;
+}
+
 // Launch one admitted group on its slot: copy every X in, run one batched
 // launch over the group's graphs, copy every Y out, then signal completion.
 static cola_status launch_group(cola_server *S, Group *G)
@@ -133,6 +184,12 @@ static cola_status launch_group(cola_server *S, Group *G)
     const Request *r0 = G->reqs[0];
     const size_t xs = r0->xdt == COLA_FLOAT32 ? 4 : 2, ys = r0->ydt == COLA_FLOAT32 ? 4 : 2;
     int64_t items = 0, hub = 0;
+    // a small group moves its bytes with the SMs when every host buffer allows it
+    bool by_sms = G->small && S->sm_copies && sm_copy_ok(sl.h_desc, sl.d_desc, 16);
+    for (const Request *r : G->reqs)
+        by_sms = by_sms && ((r->rows * r->K * (int64_t)xs) % 16) == 0 && ((r->rows * r->K * (int64_t)ys) % 16) == 0 &&
+                 sm_copy_ok(r->X_host, r->X_host, 16) && sm_copy_ok(r->Y_host, r->Y_host, 16);
+    G->by_sms = by_sms;
     COLA_CUDA(cudaEventRecord(sl.ev[0], st));
     for (int i = 0; i < n; i++) {
         Request *r = G->reqs[(size_t)i];
@@ -141,8 +198,11 @@ static cola_status launch_group(cola_server *S, Group *G)
         COLA_CUDA(cudaMallocFromPoolAsync(&r->dY, (size_t)r->rows * r->K * ys, S->pool, st));
         if (g->nseg > 0)
             COLA_CUDA(cudaMallocFromPoolAsync((void **)&r->dws, (size_t)g->nseg * r->K * sizeof(float), S->pool, st));
-        COLA_TRY(copy_chunked(r->dX, r->X_host, (size_t)r->rows * r->K * xs, cudaMemcpyHostToDevice,
-                              S->copy_chunk, st));
+        if (by_sms)
+            COLA_TRY(copy_by_sms(r->dX, r->X_host, (size_t)r->rows * r->K * xs, false, st));
+        else
+            COLA_TRY(copy_chunked(r->dX, r->X_host, (size_t)r->rows * r->K * xs, cudaMemcpyHostToDevice,
+                                  S->copy_chunk, st));
         BatchGraph &d = sl.h_desc[i];
         fill_batch_graph(d, g, r->dX, r->K, r->dY, r->K, r->K, r->xdt, r->dws);
         d.item0 = items;
@@ -151,7 +211,10 @@ static cola_status launch_group(cola_server *S, Group *G)
         hub += g->nhub * ((r->K + 127) / 128);
     }
     COLA_CUDA(cudaEventRecord(sl.ev[1], st));
-    COLA_CUDA(cudaMemcpyAsync(sl.d_desc, sl.h_desc, (size_t)n * sizeof(BatchGraph), cudaMemcpyHostToDevice, st));
+    if (by_sms && ((size_t)n * sizeof(BatchGraph)) % 16 == 0)
+        COLA_TRY(copy_by_sms(sl.d_desc, sl.h_desc, (size_t)n * sizeof(BatchGraph), false, st));
+    else
+        COLA_CUDA(cudaMemcpyAsync(sl.d_desc, sl.h_desc, (size_t)n * sizeof(BatchGraph), cudaMemcpyHostToDevice, st));
     BatchLaunch L;
     L.desc = sl.d_desc;
     L.ngraphs = n;
@@ -165,9 +228,13 @@ static cola_status launch_group(cola_server *S, Group *G)
     L.accumulate = 0;
     COLA_TRY(launch_batch(L, st));
     COLA_CUDA(cudaEventRecord(sl.ev[2], st));
-    for (Request *r : G->reqs)
-        COLA_TRY(copy_chunked(r->Y_host, r->dY, (size_t)r->rows * r->K * ys, cudaMemcpyDeviceToHost,
-                              S->copy_chunk, st));
+    for (Request *r : G->reqs) {
+        if (by_sms)
+            COLA_TRY(copy_by_sms(r->Y_host, r->dY, (size_t)r->rows * r->K * ys, true, st));
+        else
+            COLA_TRY(copy_chunked(r->Y_host, r->dY, (size_t)r->rows * r->K * ys, cudaMemcpyDeviceToHost,
+                                  S->copy_chunk, st));
+    }
     COLA_CUDA(cudaEventRecord(sl.ev[3], st));
     for (Request *r : G->reqs) {
         COLA_CUDA(cudaFreeAsync(r->dX, st));
@@ -287,6 +354,7 @@ cola_status cola_server_create(const cola_server_opts *opts, cola_server **out)
     S->group_bytes = (int64_t)(opts && opts->group_mib > 0 ? opts->group_mib : 32) << 20;
     S->small_bytes = opts && opts->small_mib < 0 ? 0 : (int64_t)(opts && opts->small_mib > 0 ? opts->small_mib : 16) << 20;
     S->copy_chunk = (int64_t)(opts && opts->copy_chunk_mib > 0 ? opts->copy_chunk_mib : 32) << 20;
+    S->sm_copies = !(opts && opts->copy_engines_only);
     cudaMemPoolProps pp;
     std::memset(&pp, 0, sizeof(pp));
     pp.allocType = cudaMemAllocationTypePinned;

@@ -44,6 +44,7 @@ struct SchedGroup {
     int64_t bytes = 0;
     bool completed = false;
     bool small = false;  // opened by a small request (size classes)
+    bool by_sms = false;  // its copies run as kernels (the server's small groups)
     bool timed = false;
     float ms[3] = {0, 0, 0};  // copy-in, launch, copy-out (read when retired)
 };

@@ -34,11 +34,13 @@ class Request:
 
 
 class Server:
-    def __init__(self, memory_budget=0, slots=0, max_group=0, group_mib=0, small_mib=0, copy_chunk_mib=0):
+    def __init__(self, memory_budget=0, slots=0, max_group=0, group_mib=0, small_mib=0, copy_chunk_mib=0,
+                 copy_engines_only=False):
         """small_mib: requests with at most this many MiB of copies are small
         (a slot is kept for them and they may pass a large request that waits;
         0 = 16, -1 = plain FIFO).  copy_chunk_mib: copies move in pieces of at
-        most this size (0 = 32)."""
+        most this size (0 = 32).  copy_engines_only: small groups copy with the
+        copy engines too, instead of with a kernel on pinned host memory."""
         o = ServerOpts()
         o.memory_budget = int(memory_budget)
         o.slots = int(slots)
@@ -46,6 +48,7 @@ class Server:
         o.group_mib = int(group_mib)
         o.small_mib = int(small_mib)
         o.copy_chunk_mib = int(copy_chunk_mib)
+        o.copy_engines_only = 1 if copy_engines_only else 0
         h = ctypes.c_void_p()
         check(lib().cola_server_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h

@@ -567,7 +567,11 @@ typedef struct cola_server_opts {
                                0 = 16; -1 = no size classes (plain FIFO) */
     int32_t copy_chunk_mib; /* copies move in pieces of at most this many MiB, so that another
                                slot's copies can run between the pieces of a long one; 0 = 32 */
-    int32_t reserved[1];
+    int32_t copy_engines_only; /* 0: a small group's copies (and its launch descriptors) are made by
+                                  a kernel reading and writing the pinned host buffers directly, so
+                                  they do not queue behind other slots' copies in the copy engines
+                                  (used when every host buffer is pinned, device-addressable and
+                                  16-byte aligned); 1: every copy by the copy engines */
 } cola_server_opts;
 
 /* Create a server on the current device (opts may be NULL).  A scheduler

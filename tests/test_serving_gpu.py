@@ -147,3 +147,29 @@ def test_register_device_built_graph(graphs):
         srv.register_graph(g)
     assert g.handle is None
     srv.close()
+
+
+def test_small_requests_copied_by_sms_equal_copy_engines(graphs):
+    """Small groups move their bytes with a kernel on the pinned host buffers
+    (not queued behind other slots' copies in the copy engines): the results
+    are the bits the copy-engine path gives, in a mix with a large request,
+    and pageable host buffers still work (they take the copy engines)."""
+    n, row, col, val, ps = graphs[4]
+    big_n, _, _, _, big_ps = graphs[2]
+    results = []
+    for engines_only in (False, True):
+        srv = Server(slots=3, max_group=4, small_mib=16, copy_engines_only=engines_only)
+        gid = srv.register(ps)
+        gbig = srv.register(big_ps)
+        xs = [host_x(n, K, seed=K) for K in (16, 64, 128)]
+        big = srv.submit(gbig, host_x(big_n, 512, seed=3), out_dtype=torch.float32)
+        reqs = [srv.submit(gid, x) for x in xs]
+        pageable = torch.from_numpy(dense_x(n, 32, 11))  # not pinned
+        rp = srv.submit(gid, pageable)
+        results.append([r.wait(timeout_ms=120000).clone() for r in reqs] + [rp.wait(timeout_ms=120000).clone()])
+        big.wait(timeout_ms=120000)
+        srv.close()
+    for a, b in zip(results[0], results[1]):
+        assert torch.equal(a, b)
+    ref = fp64_reference(n, row, col, val, dense_x(n, 64, 64))
+    assert rel(results[0][1].numpy(), ref) <= TOL_F32
