@@ -556,7 +556,7 @@ def run_ours(args, w):
     phys = traffic if traffic is not None else compulsory
     achieved = phys / k_s / 1e9
     alg_achieved = B / k_s / 1e9
-    ceil = gather_ceilings(stream) if not overridden else {"l2": None, "dram": None}
+    ceil = gather_ceilings(stream) if not (overridden or args.no_extras) else {"l2": None, "dram": None}
     gather_bytes = int(info.nnz) * K * s_x  # the X rows the entries name (the gathers)
     launches_per_step = int(g.get_info().last_launches)  # counted by the library
     line = {
