@@ -613,6 +613,14 @@ def run_ours(args, w):
         "clocks": clk,
     }
     extras = world == 1 and not args.no_extras and not overridden
+    if extras and eff == S.SCHEDULE_ROWS:
+        # the project's autotuner on these operands: its choice among the launch options
+        # (every candidate gives the same bits), beside the default launch's time
+        opts_t, ms_t, _ = g.autotune(X, Y, reps=3, stream=stream)
+        line["autotuned"] = {"choice": {k: v for k, v in opts_t.items() if k != "gather_batch_rows"},
+                             "ms": ms_t, "default_kernel_ms_median": k_med,
+                             "searched": "feature tile per pass x loads in flight x resident blocks per SM "
+                                         "(cola_spmm_autotune)"}
     if extras and xdt == torch.bfloat16:
         # the plain FP32 path on the identical graph and features
         X32 = torch.from_numpy(Xh).to(dev)
