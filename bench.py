@@ -189,6 +189,10 @@ class Clocks:
 def make_graph(w):
     import cola_b200 as cb
     n, row, col, val = cb.rmat(w["scale"], w["deg"], w["seed"])
+    if w.get("reorder") == "community":
+        # the reference's reordering step before partitioning (rabbit_order_write.py:48-55)
+        mapping, _ = cb.community_order(n, row, col)
+        row, col = cb.relabel_edges(n, row, col, mapping)
     return n, row, col, val
 
 
@@ -545,7 +549,7 @@ def run_ours(args, w):
     err, nsamp, longest = fp64_error(n, row, col, val, Xh, Y, dev)
     peak, peak_kind = measured_peak()
     compulsory = int(info.nnz) * 8 + n * K * (s_x + s_y)
-    overridden = args.scale is not None or args.K is not None
+    overridden = args.scale is not None or args.K is not None or args.reorder != "none"
     if eff == S.SCHEDULE_ROWS and not overridden:
         traffic, traffic_src = profiled_traffic(args.workload, opts_key(args))
     else:
@@ -1451,6 +1455,8 @@ def main():
                     help="default workload: open-loop length of its serving leg")
     ap.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
     ap.add_argument("--K", type=int, default=None, help="override the feature width (exploration runs)")
+    ap.add_argument("--reorder", default="none", choices=["none", "community"],
+                    help="relabel the graph by cola_community_order before partitioning (exploration runs)")
     args = ap.parse_args()
     if args.workload == "prep":
         return run_prep_reference(args) if args.impl == "reference" else run_prep(args)
@@ -1467,6 +1473,9 @@ def main():
     if args.K is not None:
         w["K"] = args.K
         w["desc"] = "{} [K overridden to {}]".format(w["desc"], args.K)
+    if args.reorder != "none":
+        w["reorder"] = args.reorder
+        w["desc"] = "{} [vertices in community order]".format(w["desc"])
     if args.impl == "reference":
         return run_reference(args, w)
     return run_ours(args, w)

@@ -7,11 +7,11 @@ sm_100a CUDA kernels behind the C ABI in include/cola_spmm.h.
 """
 from . import _lib
 from ._lib import ColaError, lib  # noqa: F401
-from .prep import (PartitionSet, bin2vec, global_csr, nnz_split, nnz_split_device, ppl_row_partition,  # noqa: F401
-                   relabel_edges, rmat, row_partition, serialize, stage_tables, workgroup_cols, write_bin)
+from .prep import (PartitionSet, bin2vec, community_order, global_csr, nnz_split, nnz_split_device,  # noqa: F401
+                   ppl_row_partition, relabel_edges, rmat, row_partition, serialize, stage_tables, workgroup_cols, write_bin)
 
 __all__ = ["PartitionSet", "row_partition", "serialize", "ppl_row_partition", "nnz_split", "nnz_split_device",
-           "relabel_edges", "stage_tables",
+           "relabel_edges", "community_order", "stage_tables",
            "workgroup_cols", "global_csr", "bin2vec", "write_bin", "rmat", "ColaError", "lib", "version"]
 
 

@@ -113,6 +113,7 @@ SIGNATURES = {
     "cola_graph_build_device": (I32, [I32, I64, P, P, P, I32, P, P, P]),
     "cola_nnz_split_device": (I32, [P, I64, P, I64, P, P, I64, P, P]),
     "cola_relabel_edges": (I32, [I32, I64, P, P, P, P, P]),
+    "cola_community_order": (I32, [I32, I64, P, P, P, P]),
     "cola_relabel_edges_device": (I32, [I32, I64, P, P, P, P, P, P]),
     "cola_global_csr": (I32, [I32, I64, P, P, P, P, P, P, P]),
     "cola_workgroup_cols": (I32, [I32, I64, P, P, I32, I32, I32, P, P]),

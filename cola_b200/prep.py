@@ -255,6 +255,21 @@ def relabel_edges(num_nodes, row, col, mapping):
     return out_r, out_c
 
 
+def community_order(num_nodes, row, col):
+    """The reordering step run before partitioning (rabbit_order_write.py:48-55;
+    cola_community_order): communities by incremental aggregation, numbered
+    community by community.  Returns (mapping old -> new, communities); with
+    relabel_edges it gives the reordered edge list rabbit.reorder returns."""
+    row = _i32(row)
+    col = _i32(col)
+    if len(row) != len(col):
+        raise ValueError("row and col differ in length")
+    mapping = np.empty(int(num_nodes), np.int32)
+    nc = ctypes.c_int64()
+    check(lib().cola_community_order(int(num_nodes), len(row), _p(row), _p(col), _p(mapping), ctypes.byref(nc)))
+    return mapping, nc.value
+
+
 def stage_tables(me, nranks, group_size, num_nodes, csc_colIdx_zip_r, nchunks_l, wg_lists):
     """src/distSpMM_ppl_batch.cu:101-193 for PE `me`."""
     nstages = nranks // group_size

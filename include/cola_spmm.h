@@ -132,6 +132,20 @@ cola_status cola_relabel_edges_device(int32_t num_nodes, int64_t nnz, const int3
                                       const int32_t *mapping, int32_t *out_row, int32_t *out_col,
                                       cola_stream_t stream);
 
+/* The reordering step the reference runs before partitioning
+ * (rabbit_order_write.py:48-55 calls its Rabbit Order module,
+ * rabbit_module/src/reorder.cpp:260-288), written from the published method:
+ * communities found by incremental aggregation (vertices visited by increasing
+ * degree, each merged into the neighbouring community of largest positive
+ * modularity gain), then numbered community by community, each community's
+ * merge tree depth first, so that its vertices get consecutive ids.  The COO is
+ * read as an undirected graph (self-loops ignored, duplicates adding up).
+ * mapping[old] = new (a permutation of 0..num_nodes-1, for
+ * cola_relabel_edges); *communities (may be NULL) receives the number of
+ * top-level communities.  Deterministic; host only. */
+cola_status cola_community_order(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
+                                 int32_t *mapping, int64_t *communities);
+
 /* prep_torch_par.py:93-101 (serialize: global CSR).  rowPtr: num_nodes+1;
  * colIdx/val: capacity nnz (val may be NULL). */
 cola_status cola_global_csr(int32_t num_nodes, int64_t nnz, const int32_t *row, const int32_t *col,
