@@ -193,6 +193,8 @@ def make_graph(w):
         # the reference's reordering step before partitioning (rabbit_order_write.py:48-55)
         mapping, _ = cb.community_order(n, row, col)
         row, col = cb.relabel_edges(n, row, col, mapping)
+        order = np.lexsort((col, row))  # sorted by (row, col) again, as the accuracy check reads it
+        row, col, val = row[order], col[order], val[order]
     return n, row, col, val
 
 
