@@ -563,6 +563,14 @@ def run_ours(args, w):
     achieved = phys / k_s / 1e9
     alg_achieved = B / k_s / 1e9
     ceil = gather_ceilings(stream) if not (overridden or args.no_extras) else {"l2": None, "dram": None}
+    pattern = {"gbps": None, "ms": None}
+    if eff == S.SCHEDULE_ROWS and not args.no_extras:
+        import ctypes
+        v, t = ctypes.c_double(), ctypes.c_float()
+        if cb.lib().cola_probe_graph_gather(g._h, ctypes.c_void_p(X.data_ptr()), X.stride(0) * s_x, K * s_x, 5,
+                                            ctypes.c_void_p(stream.cuda_stream), ctypes.byref(v),
+                                            ctypes.byref(t)) == 0:
+            pattern = {"gbps": v.value, "ms": t.value}
     gather_bytes = int(info.nnz) * K * s_x  # the X rows the entries name (the gathers)
     launches_per_step = int(g.get_info().last_launches)  # counted by the library
     line = {
@@ -600,9 +608,14 @@ def run_ours(args, w):
                                 "l2_ceiling": ceil["l2"], "dram_ceiling": ceil["dram"],
                                 "frac_of_l2_ceiling": None if not ceil["l2"] else
                                 gather_bytes / k_s / 1e9 / ceil["l2"],
+                                # the same gathers in the same order with no arithmetic and no writes
+                                "pattern_ceiling": pattern["gbps"], "pattern_ms": pattern["ms"],
+                                "frac_of_pattern_ceiling": None if not pattern["gbps"] else
+                                gather_bytes / k_s / 1e9 / pattern["gbps"],
                                 "unit": "GB/s",
                                 "note": "ceilings: 512-byte rows at random indices from a 16 MiB table (L2) and "
-                                        "a 4 GiB table (DRAM), 4 rows in flight per warp, one full wave"}},
+                                        "a 4 GiB table (DRAM), 4 rows in flight per warp, one full wave; "
+                                        "pattern: this graph's own entries in order (cola_probe_graph_gather)"}},
         "e2e": None if e2e_ms is None else {
             "value": B * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": n * K * s_x,
             "d2h_bytes_per_step": n * K * s_y, "ms_per_step": e2e_ms,

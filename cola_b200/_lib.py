@@ -109,6 +109,7 @@ SIGNATURES = {
     "cola_set_gather_bulk": (I32, [I32]),
     "cola_set_gather_wait_limit": (I32, [I64]),
     "cola_probe_gather": (I32, [I64, I32, I64, I32, P, P]),
+    "cola_probe_graph_gather": (I32, [P, P, I64, I32, I32, P, P, P]),
     "cola_device_error_check": (I32, [P]),
     "cola_graph_build_device": (I32, [I32, I64, P, P, P, I32, P, P, P]),
     "cola_nnz_split_device": (I32, [P, I64, P, I64, P, P, I64, P, P]),

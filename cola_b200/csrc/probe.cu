@@ -64,6 +64,44 @@ __global__ void __launch_bounds__(256) gather_probe_kernel(const uint4 *__restri
         sink[warp] = (float)acc;
 }
 
+// The graph's own access pattern without the arithmetic: warps walk the row
+// view's entries in order, 32 at a time (as the streaming kernel's tasks do),
+// and read the X row each entry names -- `vecs` 16-byte vectors per lane,
+// 4 rows in flight -- keeping only an XOR of the data.  Its time is the
+// memory system's time for exactly the SpMM's gathers.
+__global__ void __launch_bounds__(256) graph_gather_kernel(const char *__restrict__ X, int64_t ld_bytes,
+                                                           const int32_t *__restrict__ col, int64_t nnz, int vecs,
+                                                           int row_vecs, float *__restrict__ sink)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int64_t nwarps = (int64_t)gridDim.x * 8;
+    uint32_t acc = 0;
+    for (int64_t e0 = warp * 32; e0 < nnz; e0 += nwarps * 32) {
+        const int n = (int)min((int64_t)32, nnz - e0);
+        const int32_t mine = lane < n ? __ldcs(col + e0 + lane) : 0;
+        for (int j = 0; j < n; j += 4) {
+            uint4 v[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int32_t r = __shfl_sync(0xffffffffu, mine, (j + u) & 31);
+                const uint4 *p = reinterpret_cast<const uint4 *>(X + (int64_t)r * ld_bytes);
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    v[u][q] = (j + u < n && q < vecs && lane + 32 * q < row_vecs) ? __ldg(p + lane + 32 * q)
+                                                                                  : make_uint4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    acc += v[u][q].x ^ v[u][q].y ^ v[u][q].z ^ v[u][q].w;
+        }
+    }
+    if (acc == 0x9e3779b9u)  // practically never: keeps the loads alive
+        sink[warp] = (float)acc;
+}
+
 }  // namespace probe
 }  // namespace cola
 
@@ -123,5 +161,55 @@ extern "C" cola_status cola_probe_gather(int64_t table_bytes, int32_t row_bytes,
     COLA_CUDA(e);
     COLA_CUDA(cudaStreamSynchronize(st));
     *gbps = (double)gathers * row_bytes * reps / (ms * 1e-3) / 1e9;
+    return COLA_SUCCESS;
+}
+
+extern "C" cola_status cola_probe_graph_gather(const cola_graph *g, const void *X, int64_t ld_bytes,
+                                               int32_t row_bytes, int32_t reps, cola_stream_t stream, double *gbps,
+                                               float *ms_per_pass)
+{
+    COLA_REQUIRE(g && g->has_rows && X && gbps && row_bytes >= 16 && row_bytes <= 2048 && row_bytes % 16 == 0 &&
+                     ld_bytes >= row_bytes && ld_bytes % 16 == 0 && ((uintptr_t)X & 15u) == 0 && reps >= 1,
+                 COLA_ERROR_INVALID_ARGUMENT,
+                 "cola_probe_graph_gather: a graph with its row view, X 16-byte aligned, rows of 16..2048 bytes "
+                 "(a multiple of 16) at a stride of at least that many");
+    cudaStream_t st = (cudaStream_t)stream;
+    int64_t nnz = 0;
+    COLA_CUDA(cudaMemcpyAsync(&nnz, g->rv_ptr + g->N, sizeof nnz, cudaMemcpyDeviceToHost, st));
+    COLA_CUDA(cudaStreamSynchronize(st));
+    const int row_vecs = row_bytes / 16, vecs = (row_vecs + 31) / 32;
+    const int blocks = sm_count() * blocks_per_sm((const void *)probe::graph_gather_kernel, 256);
+    float *sink = nullptr;
+    COLA_CUDA(cudaMallocAsync((void **)&sink, (size_t)blocks * 8 * sizeof(float), st));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&e1);
+    float ms = 0.f;
+    for (int pass = 0; pass < 2 && e == cudaSuccess; pass++) {  // pass 0 warms the cache
+        e = cudaEventRecord(e0, st);
+        for (int r = 0; r < (pass ? reps : 1) && e == cudaSuccess; r++) {
+            probe::graph_gather_kernel<<<blocks, 256, 0, st>>>(static_cast<const char *>(X), ld_bytes, g->rv_col, nnz,
+                                                               vecs, row_vecs, sink);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess)
+            e = cudaEventRecord(e1, st);
+        if (e == cudaSuccess)
+            e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess && pass)
+            e = cudaEventElapsedTime(&ms, e0, e1);
+    }
+    if (e0)
+        cudaEventDestroy(e0);
+    if (e1)
+        cudaEventDestroy(e1);
+    cudaFreeAsync(sink, st);
+    COLA_CUDA(e);
+    COLA_CUDA(cudaStreamSynchronize(st));
+    ms /= reps;
+    *gbps = (double)nnz * row_bytes / (ms * 1e-3) / 1e9;
+    if (ms_per_pass)
+        *ms_per_pass = ms;
     return COLA_SUCCESS;
 }

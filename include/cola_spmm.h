@@ -406,6 +406,16 @@ cola_status cola_set_gather_wait_limit(int64_t polls);
 cola_status cola_probe_gather(int64_t table_bytes, int32_t row_bytes, int64_t gathers, int32_t reps,
                               cola_stream_t stream, double *gbps);
 
+/* The same ceiling for one graph's own access pattern: warps walk the row
+ * view's entries in order, 32 at a time, and read the row_bytes (16..2048) of X
+ * each entry names (rows ld_bytes apart), with no arithmetic and no writes.
+ * *gbps = entries x row_bytes per second over `reps` passes after a warm-up
+ * pass; *ms_per_pass (may be NULL) the time of one pass.  The SpMM kernel's
+ * time against this one is its overhead over the memory system's time for
+ * exactly its gathers.  Synchronises `stream`. */
+cola_status cola_probe_graph_gather(const cola_graph *g, const void *X, int64_t ld_bytes, int32_t row_bytes,
+                                    int32_t reps, cola_stream_t stream, double *gbps, float *ms_per_pass);
+
 /* Waits for the current device, then reports (and clears) the error code a
  * kernel left when one of its bounded waits ran out: 0 = none; 1 = a bulk-copy
  * gather stopped early (it drained every copy it had issued before exiting);
