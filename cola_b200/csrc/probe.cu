@@ -65,36 +65,42 @@ __global__ void __launch_bounds__(256) gather_probe_kernel(const uint4 *__restri
 }
 
 // The graph's own access pattern without the arithmetic: warps walk the row
-// view's entries in order, 32 at a time (as the streaming kernel's tasks do),
-// and read the X row each entry names -- `vecs` 16-byte vectors per lane,
-// 4 rows in flight -- keeping only an XOR of the data.  Its time is the
+// view's entries in order, 32 at a time (as the streaming kernel's tasks do,
+// the next 32 indices loading while these are used), and read the X row each
+// entry names -- VECS 16-byte vectors per lane, 4 rows in flight -- keeping
+// only an XOR of the data.  Its time is the
 // memory system's time for exactly the SpMM's gathers.
+template <int VECS>
 __global__ void __launch_bounds__(256) graph_gather_kernel(const char *__restrict__ X, int64_t ld_bytes,
-                                                           const int32_t *__restrict__ col, int64_t nnz, int vecs,
+                                                           const int32_t *__restrict__ col, int64_t nnz,
                                                            int row_vecs, float *__restrict__ sink)
 {
     const int lane = threadIdx.x & 31;
     const int64_t warp = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
     const int64_t nwarps = (int64_t)gridDim.x * 8;
     uint32_t acc = 0;
+    // the next batch of indices is loaded while this one's rows are read
+    int32_t next = warp * 32 + lane < nnz ? __ldcs(col + warp * 32 + lane) : 0;
     for (int64_t e0 = warp * 32; e0 < nnz; e0 += nwarps * 32) {
         const int n = (int)min((int64_t)32, nnz - e0);
-        const int32_t mine = lane < n ? __ldcs(col + e0 + lane) : 0;
+        const int32_t mine = next;
+        const int64_t e1 = e0 + nwarps * 32 + lane;
+        next = e1 < nnz ? __ldcs(col + e1) : 0;
         for (int j = 0; j < n; j += 4) {
-            uint4 v[4][4];
+            uint4 v[4][VECS];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int32_t r = __shfl_sync(0xffffffffu, mine, (j + u) & 31);
                 const uint4 *p = reinterpret_cast<const uint4 *>(X + (int64_t)r * ld_bytes);
 #pragma unroll
-                for (int q = 0; q < 4; q++)
-                    v[u][q] = (j + u < n && q < vecs && lane + 32 * q < row_vecs) ? __ldg(p + lane + 32 * q)
-                                                                                  : make_uint4(0, 0, 0, 0);
+                for (int q = 0; q < VECS; q++)
+                    v[u][q] = (j + u < n && lane + 32 * q < row_vecs) ? __ldg(p + lane + 32 * q)
+                                                                      : make_uint4(0, 0, 0, 0);
             }
 #pragma unroll
             for (int u = 0; u < 4; u++)
 #pragma unroll
-                for (int q = 0; q < 4; q++)
+                for (int q = 0; q < VECS; q++)
                     acc += v[u][q].x ^ v[u][q].y ^ v[u][q].z ^ v[u][q].w;
         }
     }
@@ -178,7 +184,9 @@ extern "C" cola_status cola_probe_graph_gather(const cola_graph *g, const void *
     COLA_CUDA(cudaMemcpyAsync(&nnz, g->rv_ptr + g->N, sizeof nnz, cudaMemcpyDeviceToHost, st));
     COLA_CUDA(cudaStreamSynchronize(st));
     const int row_vecs = row_bytes / 16, vecs = (row_vecs + 31) / 32;
-    const int blocks = sm_count() * blocks_per_sm((const void *)probe::graph_gather_kernel, 256);
+    auto fn = vecs == 1 ? probe::graph_gather_kernel<1> : vecs == 2 ? probe::graph_gather_kernel<2>
+                                                                    : probe::graph_gather_kernel<4>;
+    const int blocks = sm_count() * blocks_per_sm((const void *)fn, 256);
     float *sink = nullptr;
     COLA_CUDA(cudaMallocAsync((void **)&sink, (size_t)blocks * 8 * sizeof(float), st));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -189,8 +197,7 @@ extern "C" cola_status cola_probe_graph_gather(const cola_graph *g, const void *
     for (int pass = 0; pass < 2 && e == cudaSuccess; pass++) {  // pass 0 warms the cache
         e = cudaEventRecord(e0, st);
         for (int r = 0; r < (pass ? reps : 1) && e == cudaSuccess; r++) {
-            probe::graph_gather_kernel<<<blocks, 256, 0, st>>>(static_cast<const char *>(X), ld_bytes, g->rv_col, nnz,
-                                                               vecs, row_vecs, sink);
+            fn<<<blocks, 256, 0, st>>>(static_cast<const char *>(X), ld_bytes, g->rv_col, nnz, row_vecs, sink);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess)
