@@ -133,6 +133,7 @@ void fill_batch_graph(BatchGraph &d, const cola_graph *g, const void *X, int64_t
     d.ba.seg_beg = g->seg_beg;
     d.ba.nseg = g->nseg;
     d.ba.seg_len = g->hub_segment;
+    d.ba.queue = nullptr;  // the batch kernel assigns items statically
     d.ba.ws = ws;
     d.ba.ld_ws = K;
     d.X = X;

@@ -91,6 +91,9 @@ struct cola_graph {
     int64_t nseg = 0, nhub = 0, ntask = 0;
     int32_t hub_threshold = 256, hub_segment = 256, task_entries = 256;
     float *ws_hub = nullptr;  // nseg x K partials
+    // dev::kMaxItemQueues + 1 work-item counters of the row-major schedule,
+    // in dmem, zero between launches
+    unsigned long long *item_queue = nullptr;
     size_t ws_hub_bytes = 0;
     cola::HostPipe *host_pipe = nullptr;  // created by the first cola_spmm_host call
 };

@@ -379,6 +379,17 @@ static cola_status launch_block_t(const dev::BlockArgs &ba, const RowsLaunch &a,
             return COLA_SUCCESS;
         }
     }
+    if (ba.queue && ntile <= dev::kMaxItemQueues) {
+        // items drawn from the graph's counters: a warp that met slow items draws fewer
+        auto fn = dev::rowblock_spmm_kernel<TR, TY, LG, NV, UNROLL, VEC, MINB, true>;
+        const int64_t gx = grid_for((const void *)fn, ba.nseg + ba.ntask);
+        t_launches++;
+        fn<<<dim3((unsigned)gx, (unsigned)ntile), dev::kThreads, 0, st>>>(ba, static_cast<const T *>(a.X), a.ldx,
+                                                                          static_cast<TY *>(a.Y), a.ldy, a.K,
+                                                                          a.accumulate);
+        COLA_CUDA(cudaGetLastError());
+        return COLA_SUCCESS;
+    }
     auto fn = dev::rowblock_spmm_kernel<TR, TY, LG, NV, UNROLL, VEC, MINB>;
     const int64_t gx = grid_for((const void *)fn, ba.nseg + ba.ntask);
     t_launches++;
@@ -867,7 +878,7 @@ cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *o
     }
     const size_t desc_buf = ar.add(nullptr, (size_t)P * sizeof(GatherSeg));
     size_t o_rv_ptr = 0, o_rv_col = 0, o_rv_val = 0, o_seg_row = 0, o_seg_beg = 0, o_hub_row = 0, o_hub_seg = 0;
-    size_t o_task_rb = 0, o_task_re = 0;
+    size_t o_task_rb = 0, o_task_re = 0, o_queue = 0;
     if (rows) {
         o_rv_ptr = ar.add(rv.ptr.data(), rv.ptr.size() * 8);
         o_rv_col = ar.add(rv.col.data(), rv.col.size() * 4);
@@ -878,6 +889,7 @@ cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *o
         o_hub_seg = ar.add(rv.hub_seg.data(), rv.hub_seg.size() * 8);
         o_task_rb = ar.add(rv.task_rb.data(), rv.task_rb.size() * 4);
         o_task_re = ar.add(rv.task_re.data(), rv.task_re.size() * 4);
+        o_queue = ar.add(nullptr, (dev::kMaxItemQueues + 1) * sizeof(unsigned long long));  // zero in the image
     }
     ar.total = std::max<size_t>(ar.total, 256);
     COLA_CUDA(cudaMalloc(&g->dmem, ar.total));
@@ -895,6 +907,7 @@ cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *o
         g->hub_seg = reinterpret_cast<const int64_t *>(base + o_hub_seg);
         g->task_rb = at(o_task_rb);
         g->task_re = at(o_task_re);
+        g->item_queue = reinterpret_cast<unsigned long long *>(base + o_queue);
     }
 
     // descriptors
@@ -1193,6 +1206,7 @@ static cola_status spmm_impl(cola_graph *g, const void *X, cola_dtype xdt, int64
             ba.seg_len = g->hub_segment;
             ba.ws = g->ws_hub;
             ba.ld_ws = K;
+            ba.queue = g->item_queue;
             COLA_TRY(launch_block(ba, a, st));
         } else {
             COLA_TRY(launch_rows(a, st));

@@ -21,6 +21,9 @@ namespace dev {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarpsPerBlock = 8;
 constexpr int kThreads = kWarpsPerBlock * 32;
+// Row-major schedule: feature tiles (gridDim.y) that can draw work items from
+// counters of their own; a graph holds kMaxItemQueues + 1 counters.
+constexpr int kMaxItemQueues = 64;
 
 // Where a remote chunk's dense row comes from.
 enum RemoteMode : int32_t {

@@ -241,6 +241,11 @@ struct BlockArgs {
     int32_t seg_len;
     float *ws;
     int64_t ld_ws;
+    // Work-item counters for the dynamic schedule (kMaxItemQueues per-tile
+    // counters, then the count of warps that have finished); all zero between
+    // launches: the last warp of a launch resets them.  NULL: static
+    // grid-stride assignment.
+    unsigned long long *queue;
 };
 
 // acc[q] += v * x[2q .. 2q+1] for one 16-byte vector of X, with the packed
@@ -273,12 +278,14 @@ __device__ __forceinline__ void fma_vec2(float2 (&acc)[TR::E / 2], float v, cons
 // BARef is `const BlockArgs` (the single-graph kernel: arguments read straight
 // from the kernel's parameter space) or `const BlockArgs &` (the batched form:
 // a descriptor in global memory).
-template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, typename BARef = const BlockArgs>
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, typename BARef = const BlockArgs,
+          bool DYN = false>
 __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, const int64_t stride,
                                                const int64_t total,
                                               const typename ElemOf<TR>::T *__restrict__ X, const int64_t ldx,
                                               TY *__restrict__ Y, const int64_t ldy, const int K, const int accumulate,
-                                              const int k0, int2 *ent, const int lg_rt = 0)
+                                              const int k0, int2 *ent, const int lg_rt = 0,
+                                              unsigned long long *queue = nullptr)
 {
     using T = typename ElemOf<TR>::T;
     using raw_t = typename TR::raw_t;
@@ -296,7 +303,22 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
         kok[j] = (k0 + (gl + j * lg) * E) < K;
     const T *xk = X + k0 + gl * E;
 
-    for (int64_t it = it0; it < total; it += stride) {
+    // DYN: items are drawn from a counter (lane 0, one item ahead, so the
+    // atomic's latency hides behind the current item); a warp that drew a
+    // slow item simply draws fewer.  Otherwise: it0, it0 + stride, ...
+    int64_t it = it0;
+    if constexpr (DYN) {
+        unsigned long long t = 0;
+        if (lane == 0)
+            t = atomicAdd(queue, 1ull);
+        it = (int64_t)__shfl_sync(kFull, t, 0);
+    }
+    while (it < total) {
+        unsigned long long next_it = 0;
+        if constexpr (DYN) {
+            if (lane == 0)
+                next_it = atomicAdd(queue, 1ull);
+        }
         const bool seg = it < ba.nseg;
         int32_t rb, re;
         int64_t e_beg;
@@ -340,15 +362,18 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
                     }
             if (g == 0) {
                 if (seg) {
+                    // the segment's FP32 partial, read once by the combine kernel
                     float *wp = ba.ws + it * ba.ld_ws + k0 + gl * E;
     #pragma unroll
                     for (int j = 0; j < NV; j++)
                         if (kok[j]) {
+                            float a[E];
     #pragma unroll
                             for (int q = 0; q < E / 2; q++) {
-                                wp[j * lg * E + 2 * q] = acc[j][q].x;
-                                wp[j * lg * E + 2 * q + 1] = acc[j][q].y;
+                                a[2 * q] = acc[j][q].x;
+                                a[2 * q + 1] = acc[j][q].y;
                             }
+                            store_out<float, E, true>(wp + j * lg * E, a, false);
                         }
                 } else {
                     TY *yp = Y + (int64_t)cur * ldy + k0 + gl * E;
@@ -456,10 +481,29 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
         }
         while (cur < re)
             flush();
+        if constexpr (DYN)
+            it = (int64_t)__shfl_sync(kFull, next_it, 0);
+        else
+            it += stride;
     }
 }
 
-template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, int MINB = 1>
+// End of a launch with the dynamic schedule: the last warp to finish puts the
+// item counters back to zero for the next launch (every warp has drawn its
+// final item before it counts itself finished).
+__device__ __forceinline__ void item_queue_release(unsigned long long *queue)
+{
+    if ((threadIdx.x & 31) == 0) {
+        const unsigned long long warps = (unsigned long long)gridDim.x * gridDim.y * kWarpsPerBlock;
+        if (atomicAdd(queue + kMaxItemQueues, 1ull) == warps - 1) {
+            for (unsigned t = 0; t < gridDim.y; t++)
+                atomicExch(queue + t, 0ull);
+            atomicExch(queue + kMaxItemQueues, 0ull);
+        }
+    }
+}
+
+template <typename TR, typename TY, int LG, int NV, int UNROLL, bool VEC_Y, int MINB = 1, bool DYN = false>
 __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __grid_constant__ BlockArgs ba,
                                                                        const typename ElemOf<TR>::T *__restrict__ X,
                                                                        int64_t ldx, TY *__restrict__ Y, int64_t ldy,
@@ -473,8 +517,11 @@ __global__ void __launch_bounds__(kThreads, MINB) rowblock_spmm_kernel(const __g
     const int k0 = blockIdx.y * W;
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
     const int64_t total = ba.nseg + ba.ntask;
-    rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y>(ba, (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5),
-                                                  nwarps, total, X, ldx, Y, ldy, K, accumulate, k0, ent);
+    rowblock_items<TR, TY, LG, NV, UNROLL, VEC_Y, const BlockArgs, DYN>(
+        ba, (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5), nwarps, total, X, ldx, Y, ldy, K, accumulate,
+        k0, ent, 0, DYN ? ba.queue + blockIdx.y : nullptr);
+    if constexpr (DYN)
+        item_queue_release(ba.queue);
 }
 
 // The same schedule with the feature tiles one after another instead of side
