@@ -1,6 +1,7 @@
 // Launchers, kernel-level C ABI and the device-resident graph of the
 // partitioned SpMM (sm_100a).
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <cstring>
 #include <memory>
@@ -513,7 +514,7 @@ bool vec_ok_rows(cola_dtype xdt, const void *X, int64_t ldx, cola_dtype ydt, con
 {
     const int E = xdt == COLA_FLOAT32 ? 4 : 8;
     const int ysz = ydt == COLA_FLOAT32 ? 4 : 2;
-    if (K % E || ldx % E || !aligned16(X))
+    if (K % E || ldx % E || ldx > INT32_MAX || !aligned16(X))
         return false;
     if (ldy % E || ((uintptr_t)Y % (uintptr_t)(E * ysz)) != 0)
         return false;

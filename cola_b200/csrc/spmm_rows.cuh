@@ -302,6 +302,7 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
     for (int j = 0; j < NV; j++)
         kok[j] = (k0 + (gl + j * lg) * E) < K;
     const T *xk = X + k0 + gl * E;
+    const int32_t ldx32 = (int32_t)ldx;  // the vector path's row stride fits 32 bits (one multiply-add per entry)
 
     // DYN: items are drawn from a counter (lane 0, one item ahead, so the
     // atomic's latency hides behind the current item); a warp that drew a
@@ -431,7 +432,7 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
                     for (int u = 0; u < UNROLL; u++) {
                         const int2 p = ent[jj + u * G + g];
                         vv[u] = __int_as_float(p.y);
-                        const T *xp = xk + (int64_t)p.x * ldx;
+                        const T *xp = xk + (int64_t)p.x * ldx32;
     #pragma unroll
                         for (int j = 0; j < NV; j++)
                             if (kok[j])
@@ -449,7 +450,7 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
                         if (idx < n) {
                             const int2 p = ent[idx];
                             vv[u] = __int_as_float(p.y);
-                            const T *xp = xk + (int64_t)p.x * ldx;
+                            const T *xp = xk + (int64_t)p.x * ldx32;
     #pragma unroll
                             for (int j = 0; j < NV; j++)
                                 if (kok[j])

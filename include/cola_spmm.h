@@ -466,7 +466,11 @@ typedef struct cola_spmm_opts {
  * read only if the caller's X has them; padding rows are never referenced),
  * ldx >= K elements; Y: N rows, ldy >= K.  x_dtype FP32 or BF16 (BF16 is
  * widened exactly and accumulated in FP32); y_dtype FP32 or BF16 (rounded
- * once, at the end).  opts may be NULL. */
+ * once, at the end).  opts may be NULL.  The ROWS schedule hands its work
+ * items (hub segments, row blocks) to warps from counters kept in the graph,
+ * and hub rows' partial sums go to a workspace of the graph: calls on one
+ * graph that overlap on the GPU (different streams or threads) race on both
+ * and must be serialised by the caller; calls on one stream are. */
 cola_status cola_spmm(cola_graph *g, const void *X, cola_dtype x_dtype, int64_t ldx, void *Y, cola_dtype y_dtype,
                       int64_t ldy, int32_t K, const cola_spmm_opts *opts, cola_stream_t stream);
 
