@@ -89,7 +89,7 @@ struct cola_graph {
     const int64_t *hub_seg = nullptr;
     const int32_t *task_rb = nullptr, *task_re = nullptr;
     int64_t nseg = 0, nhub = 0, ntask = 0;
-    int32_t hub_threshold = 256, hub_segment = 256, task_entries = 256;
+    int32_t hub_threshold = 256, hub_segment = 256, task_entries = 128;
     float *ws_hub = nullptr;  // nseg x K partials
     // dev::kMaxItemQueues + 1 work-item counters of the row-major schedule,
     // in dmem, zero between launches
@@ -100,6 +100,20 @@ struct cola_graph {
 
 namespace cola {
 void graph_release(cola_graph *g);
+
+// Row view parameters: the caller's cola_upload_opts fields where non-zero,
+// else chosen by the graph's size: T = 512 when a full wave of warps (32 per
+// SM) still draws 16 or more 512-entry items each, else 256; rows longer than
+// T entries are cut into T-entry segments, the other rows packed into row
+// blocks of about T / 2 entries.  Measured with the dynamic item schedule:
+// T = 512 is 2-5 % faster than 256 on a scale-21 R-MAT graph (94 M entries,
+// BF16 features), the same at scale 20 (31 M); on 0.5-12 M-entry graphs
+// smaller items (T = 128) were slower on the largest and faster only on the
+// smallest.
+struct RowViewParams {
+    int32_t hub_threshold, hub_segment, task_entries;
+};
+RowViewParams row_view_params(int64_t nnz, const cola_upload_opts *opts);
 // The row-view graph of an nrows x ncols COO in device memory (entries sorted
 // by (row, col), duplicates merged, hub segments and row-block tasks), for
 // the row-major schedule; ncols >= nrows.

@@ -906,9 +906,8 @@ static cola_status graph_build_device(int32_t N, int64_t nnz, const int32_t *row
                  "%s: a graph built on the device is its row view", who);
     COLA_REQUIRE(!(opts && opts->group_size > 0 && opts->group_size != nparts), COLA_ERROR_UNSUPPORTED,
                  "%s: the pipelined schedule needs the split blocks (cola_graph_upload)", who);
-    const int64_t thr = opts && opts->hub_threshold > 0 ? opts->hub_threshold : 256;
-    const int64_t seg = opts && opts->hub_segment > 0 ? opts->hub_segment : 256;
-    const int64_t te = opts && opts->task_entries > 0 ? opts->task_entries : 128;
+    const RowViewParams rp = row_view_params(nnz, opts);
+    const int64_t thr = rp.hub_threshold, seg = rp.hub_segment, te = rp.task_entries;
     const int64_t npp = ((int64_t)N + nparts - 1) / nparts;
     const int cb = bits_for(NC > 0 ? (uint64_t)NC - 1 : 0);  // column bits; rows (< N <= NC) fit in as many
 

@@ -722,6 +722,19 @@ cola_status ensure(void *&p, size_t &have, size_t need)
     return COLA_SUCCESS;
 }
 
+RowViewParams row_view_params(int64_t nnz, const cola_upload_opts *opts)
+{
+    const int64_t warps = (int64_t)sm_count() * 32;
+    int64_t t = 256;
+    while (t < 512 && 2 * t * 16 * warps <= nnz)
+        t *= 2;
+    RowViewParams p;
+    p.hub_threshold = opts && opts->hub_threshold > 0 ? opts->hub_threshold : (int32_t)t;
+    p.hub_segment = opts && opts->hub_segment > 0 ? opts->hub_segment : (int32_t)t;
+    p.task_entries = opts && opts->task_entries > 0 ? opts->task_entries : (int32_t)(t / 2);
+    return p;
+}
+
 void graph_release(cola_graph *g)
 {
     if (!g)
@@ -824,9 +837,13 @@ cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *o
     const bool rows = !(opts && opts->no_row_view);
     RowView rv;
     if (rows) {
-        g->hub_threshold = opts && opts->hub_threshold > 0 ? opts->hub_threshold : 256;
-        g->hub_segment = opts && opts->hub_segment > 0 ? opts->hub_segment : 256;
-        g->task_entries = opts && opts->task_entries > 0 ? opts->task_entries : 128;
+        int64_t nnz_all = 0;
+        for (const PartHost &ph : ps->parts)
+            nnz_all += (int64_t)ph.l_colIdx.size() + (int64_t)ph.r_rowIdx.size();
+        const RowViewParams rp = row_view_params(nnz_all, opts);
+        g->hub_threshold = rp.hub_threshold;
+        g->hub_segment = rp.hub_segment;
+        g->task_entries = rp.task_entries;
         COLA_TRY(build_row_view(*ps, g->hub_threshold, g->hub_segment, g->task_entries, rv));
         g->nseg = (int64_t)rv.seg_row.size();
         g->nhub = (int64_t)rv.hub_row.size();

@@ -4,7 +4,7 @@
 // (include/dist_spmm_ppl_batch.cuh:202-245) are expanded on the device into
 // (partition row, global column, value) entries, and the device graph build
 // turns them into the row-major view -- every row's entries in column order,
-// rows longer than 256 entries cut into segments, row-block tasks.  Built once
+// long rows cut into segments, row-block tasks (sized by the view).  Built once
 // per zip pair and chunk range; each SpMM through it is the row-major
 // schedule accumulating into the caller's output, the same sum the chunk
 // kernel computes with atomics.

@@ -275,7 +275,7 @@ cola_status cola_ppl0_batch_buffer_spmm_noalloc(float *output, const float *inpu
  * cola_ppl0_batch_spmm without the dense ones): the local CSR chunks
  * [local_row_lb, +local_row_num) and remote CSC chunks [remote_col_lb,
  * +remote_col_num) of PE peid, merged per output row in column order on the
- * device (rows of more than 256 entries split into segments).  Built once
+ * device (long rows split into segments, as cola_graph_upload does).  Built once
  * (synchronises `stream`; needs about 12 bytes of device memory per entry
  * while it runs and keeps about 8 per entry); the zip arrays are not read
  * again.  cola_zip_rows_spmm then adds the same product as
@@ -345,9 +345,11 @@ typedef struct cola_upload_opts {
     int32_t if_split;       /* nnz_split the remote CSC too (src/distSpMM_ppl_batch.cu:86-98); 1 = yes */
     int32_t group_size;     /* work-group size for the pipelined schedule; 0 or nparts = single stage */
     int32_t no_row_view;    /* 1: skip the row-major view (COLA_SCHEDULE_ROWS unavailable, less memory) */
-    int32_t hub_threshold;  /* ROWS: rows with more entries are split into segments; 0 = 256 */
-    int32_t hub_segment;    /* ROWS: entries per hub segment; 0 = 256 */
-    int32_t task_entries;   /* ROWS: entries per row-block task (one warp each); 0 = 128 */
+    int32_t hub_threshold;  /* ROWS: rows with more entries are split into segments; 0 = T */
+    int32_t hub_segment;    /* ROWS: entries per hub segment; 0 = T */
+    int32_t task_entries;   /* ROWS: entries per row-block task (one warp each); 0 = T / 2.
+                               T = 512 if nnz >= 512 x 16 x 32 x SMs (16 or more 512-entry items
+                               per warp of a full wave), else 256 */
     int32_t reserved[2];
 } cola_upload_opts;
 

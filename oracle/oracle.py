@@ -239,7 +239,7 @@ def spmm_csr_f64(rowPtr, colIdx, val, X):
     return Y
 
 
-def spmm_rows_f32_ordered(rowPtr, colIdx, val, X, hub_threshold=256, hub_segment=256):
+def spmm_rows_f32_ordered(rowPtr, colIdx, val, X, hub_threshold=512, hub_segment=512):
     """FP32 Y = A X summed in the row-major schedule's fixed order (fused
     multiply-adds in CSR order per row; rows over hub_threshold entries as
     hub_segment-entry segments added by a binary counter), to be compared bit

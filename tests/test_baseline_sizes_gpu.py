@@ -181,7 +181,7 @@ def test_config3_fp32_and_bf16_against_fp64(config3):
 @pytest.mark.parametrize("xdt,tiles", [(torch.float32, (0, 64, 128, 256)),
                                        (torch.bfloat16, (0, 64, 128, 256))])
 def test_config3_hub_rows_bitwise_and_tile_widths(config3, xdt, tiles):
-    """The 64 longest rows (each cut into 256-entry segments) equal the
+    """The 64 longest rows (each cut into 512-entry segments, the default) equal the
     oracle's restatement of the summation order bit for bit, and the whole
     output is the same bits at every feature tile width."""
     n, g, rp, ci, vv, pick, counts = config3
@@ -193,7 +193,7 @@ def test_config3_hub_rows_bitwise_and_tile_widths(config3, xdt, tiles):
         assert torch.equal(y, outs[0])
     hubs = np.argsort(counts, kind="stable")[-64:].astype(np.int64)
     sp, sc, sv = sub_csr(rp, ci, vv, hubs)
-    want = oracle.spmm_rows_f32_ordered(sp, sc, sv, Xd.float().cpu().numpy(), hub_threshold=256,
-                                        hub_segment=256)
+    want = oracle.spmm_rows_f32_ordered(sp, sc, sv, Xd.float().cpu().numpy(), hub_threshold=512,
+                                        hub_segment=512)
     got = outs[0][torch.from_numpy(hubs).to(DEV)].cpu().numpy()
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
