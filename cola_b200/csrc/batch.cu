@@ -2,6 +2,7 @@
 // its own dense operands and feature width, in one persistent launch (plus one
 // for hub rows), capturable in a CUDA graph; and the launch-parameter autotuner.
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -303,6 +304,8 @@ cola_status cola_batch_bind(cola_batch *b, const void *const *X, const int64_t *
                      (long long)ldx[i], (long long)ldy[i]);
         if (g->N == 0)
             continue;
+        COLA_REQUIRE(g->nseg + g->ntask < INT32_MAX, COLA_ERROR_UNSUPPORTED,
+                     "cola_batch_bind: graph %zu has %lld work items (2^31 at most)", i, (long long)(g->nseg + g->ntask));
         if (g->nseg > 0)
             COLA_TRY(ensure(reinterpret_cast<void *&>(g->ws_hub), g->ws_hub_bytes,
                             (size_t)g->nseg * K[i] * sizeof(float)));

@@ -93,7 +93,7 @@ struct cola_graph {
     float *ws_hub = nullptr;  // nseg x K partials
     // dev::kMaxItemQueues + 1 work-item counters of the row-major schedule,
     // in dmem, zero between launches
-    unsigned long long *item_queue = nullptr;
+    unsigned int *item_queue = nullptr;
     size_t ws_hub_bytes = 0;
     cola::HostPipe *host_pipe = nullptr;  // created by the first cola_spmm_host call
 };

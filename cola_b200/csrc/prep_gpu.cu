@@ -1019,7 +1019,7 @@ static cola_status graph_build_device(int32_t N, int64_t nnz, const int32_t *row
     const size_t o_srow = place((size_t)nseg * 4), o_sbeg = place((size_t)nseg * 8);
     const size_t o_hrow = place((size_t)nhub * 4), o_hseg = place(((size_t)nhub + 1) * 8);
     const size_t o_trb = place((size_t)ntask * 4), o_tre = place((size_t)ntask * 4);
-    const size_t qbytes = (dev::kMaxItemQueues + 1) * sizeof(unsigned long long), o_q = place(qbytes);
+    const size_t qbytes = (dev::kMaxItemQueues + 1) * sizeof(unsigned int), o_q = place(qbytes);
     total = std::max<size_t>(total, 256);
     COLA_CUDA(cudaMalloc(&g->dmem, total));
     g->dbytes = total;
@@ -1059,7 +1059,7 @@ static cola_status graph_build_device(int32_t N, int64_t nnz, const int32_t *row
     g->hub_seg = reinterpret_cast<const int64_t *>(base + o_hseg);
     g->task_rb = reinterpret_cast<const int32_t *>(base + o_trb);
     g->task_re = reinterpret_cast<const int32_t *>(base + o_tre);
-    g->item_queue = reinterpret_cast<unsigned long long *>(base + o_q);
+    g->item_queue = reinterpret_cast<unsigned int *>(base + o_q);
     g->nseg = nseg;
     g->nhub = nhub;
     g->ntask = ntask;

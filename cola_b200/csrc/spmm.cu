@@ -479,6 +479,8 @@ static cola_status launch_block(const dev::BlockArgs &ba, const RowsLaunch &a, c
 {
     if (ba.nseg + ba.ntask <= 0)
         return COLA_SUCCESS;
+    COLA_REQUIRE(ba.nseg + ba.ntask < INT32_MAX, COLA_ERROR_UNSUPPORTED, "cola_spmm: %lld work items (2^31 at most)",
+                 (long long)(ba.nseg + ba.ntask));
     using BF = __nv_bfloat16;
     const int kt = rows_k_tile(a.xdt, a.K, a.k_tile);
     if (kt > 0) {
@@ -907,7 +909,7 @@ cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *o
         o_hub_seg = ar.add(rv.hub_seg.data(), rv.hub_seg.size() * 8);
         o_task_rb = ar.add(rv.task_rb.data(), rv.task_rb.size() * 4);
         o_task_re = ar.add(rv.task_re.data(), rv.task_re.size() * 4);
-        o_queue = ar.add(nullptr, (dev::kMaxItemQueues + 1) * sizeof(unsigned long long));  // zero in the image
+        o_queue = ar.add(nullptr, (dev::kMaxItemQueues + 1) * sizeof(unsigned int));  // zero in the image
     }
     ar.total = std::max<size_t>(ar.total, 256);
     COLA_CUDA(cudaMalloc(&g->dmem, ar.total));
@@ -925,7 +927,7 @@ cola_status graph_upload(const cola_partition_set *ps, const cola_upload_opts *o
         g->hub_seg = reinterpret_cast<const int64_t *>(base + o_hub_seg);
         g->task_rb = at(o_task_rb);
         g->task_re = at(o_task_re);
-        g->item_queue = reinterpret_cast<unsigned long long *>(base + o_queue);
+        g->item_queue = reinterpret_cast<unsigned int *>(base + o_queue);
     }
 
     // descriptors

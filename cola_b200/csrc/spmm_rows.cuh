@@ -245,7 +245,7 @@ struct BlockArgs {
     // counters, then the count of warps that have finished); all zero between
     // launches: the last warp of a launch resets them.  NULL: static
     // grid-stride assignment.
-    unsigned long long *queue;
+    unsigned int *queue;
 };
 
 // acc[q] += v * x[2q .. 2q+1] for one 16-byte vector of X, with the packed
@@ -285,7 +285,7 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
                                               const typename ElemOf<TR>::T *__restrict__ X, const int64_t ldx,
                                               TY *__restrict__ Y, const int64_t ldy, const int K, const int accumulate,
                                               const int k0, int2 *ent, const int lg_rt = 0,
-                                              unsigned long long *queue = nullptr)
+                                              unsigned int *queue = nullptr)
 {
     using T = typename ElemOf<TR>::T;
     using raw_t = typename TR::raw_t;
@@ -307,18 +307,21 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
     // DYN: items are drawn from a counter (lane 0, one item ahead, so the
     // atomic's latency hides behind the current item); a warp that drew a
     // slow item simply draws fewer.  Otherwise: it0, it0 + stride, ...
-    int64_t it = it0;
+    // Item numbers fit 32 bits (the launchers check nseg + ntask < 2^31): one
+    // register each, which keeps the 4-blocks-per-SM build within its 64.
+    const int32_t total32 = (int32_t)total;
+    int32_t it = (int32_t)it0;
     if constexpr (DYN) {
-        unsigned long long t = 0;
+        unsigned int t = 0;
         if (lane == 0)
-            t = atomicAdd(queue, 1ull);
-        it = (int64_t)__shfl_sync(kFull, t, 0);
+            t = atomicAdd(queue, 1u);
+        it = (int32_t)__shfl_sync(kFull, t, 0);
     }
-    while (it < total) {
-        unsigned long long next_it = 0;
+    while (it < total32) {
+        unsigned int next_it = 0;
         if constexpr (DYN) {
             if (lane == 0)
-                next_it = atomicAdd(queue, 1ull);
+                next_it = atomicAdd(queue, 1u);
         }
         const bool seg = it < ba.nseg;
         int32_t rb, re;
@@ -364,7 +367,7 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
             if (g == 0) {
                 if (seg) {
                     // the segment's FP32 partial, read once by the combine kernel
-                    float *wp = ba.ws + it * ba.ld_ws + k0 + gl * E;
+                    float *wp = ba.ws + (int64_t)it * ba.ld_ws + k0 + gl * E;
     #pragma unroll
                     for (int j = 0; j < NV; j++)
                         if (kok[j]) {
@@ -424,33 +427,32 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
                 mv = __ldcs(valp + base + 32 + lane);
             }
             for (int jj = 0; jj < n; jj += R) {
+                // the values are read from shared memory when the rows have
+                // arrived, not held in registers while the loads are in flight
                 raw_t xr[UNROLL][NV];
-                float vv[UNROLL];
                 if (jj + R <= n && base + jj + R <= row_end) {
                     // the whole round inside the current row: no boundary checks
     #pragma unroll
                     for (int u = 0; u < UNROLL; u++) {
-                        const int2 p = ent[jj + u * G + g];
-                        vv[u] = __int_as_float(p.y);
-                        const T *xp = xk + (int64_t)p.x * ldx32;
+                        const T *xp = xk + (int64_t)ent[jj + u * G + g].x * ldx32;
     #pragma unroll
                         for (int j = 0; j < NV; j++)
                             if (kok[j])
                                 xr[u][j] = TR::load(xp + j * lg * E);
                     }
     #pragma unroll
-                    for (int u = 0; u < UNROLL; u++)
+                    for (int u = 0; u < UNROLL; u++) {
+                        const float v = __int_as_float(ent[jj + u * G + g].y);
     #pragma unroll
                         for (int j = 0; j < NV; j++)
-                            fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
+                            fma_vec2<TR>(acc[j], v, xr[u][j]);
+                    }
                 } else {
     #pragma unroll
                     for (int u = 0; u < UNROLL; u++) {
                         const int idx = jj + u * G + g;
                         if (idx < n) {
-                            const int2 p = ent[idx];
-                            vv[u] = __int_as_float(p.y);
-                            const T *xp = xk + (int64_t)p.x * ldx32;
+                            const T *xp = xk + (int64_t)ent[idx].x * ldx32;
     #pragma unroll
                             for (int j = 0; j < NV; j++)
                                 if (kok[j])
@@ -468,9 +470,10 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
                         for (int u = 0; u < UNROLL; u++) {
                             const int32_t e = base + jj + u * G + g;
                             if (e >= lo && e < sh) {
+                                const float v = __int_as_float(ent[jj + u * G + g].y);
     #pragma unroll
                                 for (int j = 0; j < NV; j++)
-                                    fma_vec2<TR>(acc[j], vv[u], xr[u][j]);
+                                    fma_vec2<TR>(acc[j], v, xr[u][j]);
                             }
                         }
                         lo = sh;
@@ -483,23 +486,23 @@ __device__ __forceinline__ void rowblock_items(BARef ba, const int64_t it0, cons
         while (cur < re)
             flush();
         if constexpr (DYN)
-            it = (int64_t)__shfl_sync(kFull, next_it, 0);
+            it = (int32_t)__shfl_sync(kFull, next_it, 0);
         else
-            it += stride;
+            it += (int32_t)stride;
     }
 }
 
 // End of a launch with the dynamic schedule: the last warp to finish puts the
 // item counters back to zero for the next launch (every warp has drawn its
 // final item before it counts itself finished).
-__device__ __forceinline__ void item_queue_release(unsigned long long *queue)
+__device__ __forceinline__ void item_queue_release(unsigned int *queue)
 {
     if ((threadIdx.x & 31) == 0) {
-        const unsigned long long warps = (unsigned long long)gridDim.x * gridDim.y * kWarpsPerBlock;
-        if (atomicAdd(queue + kMaxItemQueues, 1ull) == warps - 1) {
+        const unsigned int warps = gridDim.x * gridDim.y * kWarpsPerBlock;
+        if (atomicAdd(queue + kMaxItemQueues, 1u) == warps - 1) {
             for (unsigned t = 0; t < gridDim.y; t++)
-                atomicExch(queue + t, 0ull);
-            atomicExch(queue + kMaxItemQueues, 0ull);
+                atomicExch(queue + t, 0u);
+            atomicExch(queue + kMaxItemQueues, 0u);
         }
     }
 }
