@@ -438,6 +438,29 @@ def test_rows_hub_combine_tiles_and_repeats(case12, K, thr, seg):
     assert torch.equal(outs[0], outs[1]) and torch.equal(outs[1], outs[2])
 
 
+def test_rows_item_counters_across_tile_counts(case12):
+    """Work items are drawn from counters kept in the graph (one per feature
+    tile) and put back to zero by the last warp of each launch: calls with 1,
+    2 and 4 feature tiles, interleaved on one graph, each give the right
+    result and the same bits as a fresh graph's first call."""
+    n, row, col, val, ps = case12
+    g = S.Graph(ps, hub_threshold=32, hub_segment=16)
+    assert g.info.hub_rows > 0
+    xs = {K: torch.from_numpy(dense_x(n, K, seed=K)).to(DEV) for K in (128, 1024, 2048)}
+    first = {}
+    for K in (1024, 128, 2048, 128, 1024, 2048):
+        y = g.spmm(xs[K], schedule=S.SCHEDULE_ROWS)
+        torch.cuda.synchronize()
+        if K not in first:
+            first[K] = y
+            ref = fp64_reference(n, row, col, val, xs[K].cpu().numpy())
+            assert rel(y.cpu().numpy(), ref) <= TOL_F32
+        else:
+            assert torch.equal(y, first[K])
+    fresh = S.Graph(ps, hub_threshold=32, hub_segment=16)
+    assert torch.equal(fresh.spmm(xs[2048], schedule=S.SCHEDULE_ROWS), first[2048])
+
+
 # ---------------------------------------------------------------------------
 # staged gathers by bulk asynchronous copies (TMA) vs 16-byte vectors
 # ---------------------------------------------------------------------------
