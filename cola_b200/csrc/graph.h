@@ -102,14 +102,15 @@ namespace cola {
 void graph_release(cola_graph *g);
 
 // Row view parameters: the caller's cola_upload_opts fields where non-zero,
-// else chosen by the graph's size: T = 512 when a full wave of warps (32 per
-// SM) still draws 16 or more 512-entry items each, else 256; rows longer than
-// T entries are cut into T-entry segments, the other rows packed into row
-// blocks of about T / 2 entries.  Measured with the dynamic item schedule:
-// T = 512 is 2-5 % faster than 256 on a scale-21 R-MAT graph (94 M entries,
-// BF16 features), the same at scale 20 (31 M); on 0.5-12 M-entry graphs
-// smaller items (T = 128) were slower on the largest and faster only on the
-// smallest.
+// else chosen by the graph's size: with W warps in a full wave (32 per SM),
+// T = 512 when each still draws 16 or more 512-entry items (nnz >= 512 x 16 x
+// W), T = 128 when fewer than 4 128-entry items each (nnz < 128 x 4 x W), else
+// 256; rows longer than T entries are cut into T-entry segments, the other
+// rows packed into row blocks of about T / 2 entries.  Measured with the
+// dynamic item schedule: T = 512 is 2-5 % faster than 256 on a scale-21 R-MAT
+// graph (94 M entries, BF16 features), the same at scale 20 (31 M); T = 128 is
+// faster than 256 on graphs of 0.46 and 1.4 M entries and slower at 4.4 and
+// 13 M (the per-partition views of the scale-20 graph).
 struct RowViewParams {
     int32_t hub_threshold, hub_segment, task_entries;
 };

@@ -728,7 +728,9 @@ RowViewParams row_view_params(int64_t nnz, const cola_upload_opts *opts)
 {
     const int64_t warps = (int64_t)sm_count() * 32;
     int64_t t = 256;
-    while (t < 512 && 2 * t * 16 * warps <= nnz)
+    if (nnz < 128 * 4 * warps)
+        t = 128;
+    while (t >= 256 && t < 512 && 2 * t * 16 * warps <= nnz)
         t *= 2;
     RowViewParams p;
     p.hub_threshold = opts && opts->hub_threshold > 0 ? opts->hub_threshold : (int32_t)t;

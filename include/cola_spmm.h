@@ -349,7 +349,7 @@ typedef struct cola_upload_opts {
     int32_t hub_segment;    /* ROWS: entries per hub segment; 0 = T */
     int32_t task_entries;   /* ROWS: entries per row-block task (one warp each); 0 = T / 2.
                                T = 512 if nnz >= 512 x 16 x 32 x SMs (16 or more 512-entry items
-                               per warp of a full wave), else 256 */
+                               per warp of a full wave), 128 if nnz < 128 x 4 x 32 x SMs, else 256 */
     int32_t reserved[2];
 } cola_upload_opts;
 
