@@ -20,6 +20,8 @@
 #include "tune_cache.h"
 
 using cola::dev::BatchGraph;
+static_assert(cola::kBatchQueueBytes >= (cola::dev::kMaxItemQueues + 1) * sizeof(unsigned int),
+              "the batch counters must hold the kernel's counters");
 
 struct cola_batch {
     int device = 0;
@@ -75,11 +77,14 @@ static void batch_release(cola_batch *b)
 template <typename TR, typename TY, int UNROLL, int MINB>
 static cola_status launch_batch_t(const BatchLaunch &L, cudaStream_t st)
 {
-    auto fn = dev::batch_rowblock_kernel<TR, TY, UNROLL, MINB>;
+    const bool dyn = L.queue && L.total_items < INT32_MAX;
+    auto fn = dyn ? dev::batch_rowblock_kernel<TR, TY, UNROLL, MINB, true>
+                  : dev::batch_rowblock_kernel<TR, TY, UNROLL, MINB, false>;
     int64_t gx = grid_for((const void *)fn, L.total_items);
     gx = std::max<int64_t>(1, gx * L.grid_pct / 100);
     t_launches++;
-    fn<<<(unsigned)gx, dev::kThreads, 0, st>>>(L.desc, L.ngraphs, L.total_items, L.accumulate);
+    fn<<<(unsigned)gx, dev::kThreads, 0, st>>>(L.desc, L.ngraphs, L.total_items, L.accumulate,
+                                               dyn ? L.queue : nullptr);
     COLA_CUDA(cudaGetLastError());
     return COLA_SUCCESS;
 }
@@ -166,6 +171,8 @@ static cola_status batch_run(cola_batch *b, const cola_spmm_opts *opts, cudaStre
     L.grid_pct = b->grid_pct;
     L.blocks_per_sm = b->blocks_per_sm;
     L.accumulate = accumulate;
+    L.queue = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(b->d_desc) +
+                                               batch_queue_offset(b->h_desc.size() * sizeof(BatchGraph)));
     COLA_TRY(launch_batch(L, st));
     for (const cola_batch::Solo &s : b->solo) {
         cola_spmm_opts o;
@@ -322,10 +329,13 @@ cola_status cola_batch_bind(cola_batch *b, const void *const *X, const int64_t *
         b->total_hub += g->nhub * ((K[i] + 127) / 128);
         b->h_desc.push_back(d);
     }
-    const size_t need = std::max<size_t>(b->h_desc.size(), 1) * sizeof(BatchGraph);
+    const size_t qoff = batch_queue_offset(b->h_desc.size() * sizeof(BatchGraph));
+    const size_t need = qoff + kBatchQueueBytes;
     void *p = b->d_desc;
     COLA_TRY(ensure(p, b->d_desc_bytes, need));
     b->d_desc = static_cast<BatchGraph *>(p);
+    // the work-item counters start at zero (each launch leaves them so)
+    COLA_CUDA(cudaMemsetAsync(static_cast<char *>(p) + qoff, 0, kBatchQueueBytes, st));
     if (!b->h_desc.empty())
         COLA_CUDA(cudaMemcpyAsync(b->d_desc, b->h_desc.data(), b->h_desc.size() * sizeof(BatchGraph),
                                   cudaMemcpyHostToDevice, st));

@@ -226,6 +226,8 @@ static cola_status launch_group(cola_server *S, Group *G)
     L.grid_pct = 100;
     L.blocks_per_sm = 4;
     L.accumulate = 0;
+    L.queue = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(sl.d_desc) +
+                                               batch_queue_offset((size_t)S->max_group * sizeof(BatchGraph)));
     COLA_TRY(launch_batch(L, st));
     COLA_CUDA(cudaEventRecord(sl.ev[2], st));
     for (Request *r : G->reqs) {
@@ -370,7 +372,11 @@ cola_status cola_server_create(const cola_server_opts *opts, cola_server **out)
     }
     for (Slot &sl : S->slots) {
         COLA_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
-        COLA_CUDA(cudaMalloc(&sl.d_desc, (size_t)S->max_group * sizeof(BatchGraph)));
+        // the descriptor table, then the slot's work-item counters (zero between launches;
+        // a slot's launches are ordered on its stream)
+        const size_t qoff = batch_queue_offset((size_t)S->max_group * sizeof(BatchGraph));
+        COLA_CUDA(cudaMalloc(&sl.d_desc, qoff + kBatchQueueBytes));
+        COLA_CUDA(cudaMemset(reinterpret_cast<char *>(sl.d_desc) + qoff, 0, kBatchQueueBytes));
         COLA_CUDA(cudaMallocHost(&sl.h_desc, (size_t)S->max_group * sizeof(BatchGraph)));
         sl.cap = S->max_group;
         for (cudaEvent_t &e : sl.ev)

@@ -2,7 +2,9 @@
 // persistent launch.  Work items of all graphs are concatenated (graph g owns
 // items [item0, item0 + nseg + ntask)); a warp finds its graph by advancing
 // through the descriptor table (its items only increase) and runs the item with
-// the lane geometry of that graph's width.
+// the lane geometry of that graph's width.  With DYN the items are drawn from a
+// counter (one ahead, as in the single-graph kernel): items of a K = 512 graph
+// cost 30 times those of a K = 16 one, so a static share leaves warps idle.
 #pragma once
 #include "spmm_rows.cuh"
 
@@ -36,16 +38,30 @@ inline int batch_lane_width(int K, int E)
     return lg;
 }
 
-template <typename TR, typename TY, int UNROLL, int MINB>
+template <typename TR, typename TY, int UNROLL, int MINB, bool DYN = false>
 __global__ void __launch_bounds__(kThreads, MINB) batch_rowblock_kernel(const BatchGraph *__restrict__ gs, int ng,
-                                                                     int64_t total, int accumulate)
+                                                                     int64_t total, int accumulate,
+                                                                     unsigned int *queue)
 {
     using T = typename ElemOf<TR>::T;
     __shared__ int2 s_ent[kWarpsPerBlock][32];
     int2 *ent = s_ent[threadIdx.x >> 5];
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    const int lane = threadIdx.x & 31;
     int gi = 0;
-    for (int64_t it = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); it < total; it += nwarps) {
+    int64_t it = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    if constexpr (DYN) {
+        unsigned int t = 0;
+        if (lane == 0)
+            t = atomicAdd(queue, 1u);
+        it = (int64_t)__shfl_sync(kFull, t, 0);
+    }
+    while (it < total) {
+        unsigned int next_it = 0;
+        if constexpr (DYN) {
+            if (lane == 0)
+                next_it = atomicAdd(queue, 1u);
+        }
         while (gi + 1 < ng && it >= gs[gi + 1].item0)
             gi++;
         const BatchGraph &bg = gs[gi];
@@ -55,7 +71,13 @@ __global__ void __launch_bounds__(kThreads, MINB) batch_rowblock_kernel(const Ba
             rowblock_items<TR, TY, 0, 1, UNROLL, true, const BlockArgs &>(
                 bg.ba, li, 1, li + 1, static_cast<const T *>(bg.X), bg.ldx, static_cast<TY *>(bg.Y), bg.ldy, bg.K,
                 accumulate, k0, ent, bg.lg);
+        if constexpr (DYN)
+            it = (int64_t)__shfl_sync(kFull, next_it, 0);
+        else
+            it += nwarps;
     }
+    if constexpr (DYN)
+        item_queue_release(queue);
 }
 
 template <typename TY, int UNROLL>
