@@ -438,6 +438,42 @@ def test_rows_hub_combine_tiles_and_repeats(case12, K, thr, seg):
     assert torch.equal(outs[0], outs[1]) and torch.equal(outs[1], outs[2])
 
 
+def test_row_view_sizes_follow_the_graph():
+    """Without options the row view's item size follows the graph's size: a
+    graph of a few thousand entries (far under 128 x 4 entries per warp of a
+    full wave) cuts rows longer than 128 entries into 128-entry segments, the
+    same from the host upload and the device build; options override it; the
+    product is right either way."""
+    n = 1000
+    lens = {0: 300, 1: 200, 2: 129, 3: 128}
+    rows, cols = [], []
+    for r in range(n):
+        k = lens.get(r, 1)
+        rows += [r] * k
+        cols += [(r * 7 + j * 3) % n for j in range(k)]
+    row = np.array(rows, np.int32)
+    col = np.array(cols, np.int32)
+    key = row.astype(np.int64) * n + col
+    _, first = np.unique(key, return_index=True)
+    row, col = row[np.sort(first)], col[np.sort(first)]
+    assert np.bincount(row, minlength=n)[:4].tolist() == [300, 200, 129, 128]
+    val = np.linspace(0.5, 1.5, len(row)).astype(np.float32)
+    gh = S.Graph(cb.PartitionSet.from_coo(n, row, col, val, 1))
+    gd = S.Graph.from_coo_device(n, torch.from_numpy(row).to(DEV), torch.from_numpy(col).to(DEV),
+                                 torch.from_numpy(val).to(DEV), nparts=1)
+    for g in (gh, gd):
+        assert (g.info.hub_rows, g.info.hub_segments) == (3, 3 + 2 + 2)
+    go = S.Graph(cb.PartitionSet.from_coo(n, row, col, val, 1), hub_threshold=256, hub_segment=100)
+    assert (go.info.hub_rows, go.info.hub_segments) == (1, 3)
+    X = dense_x(n, 32, seed=11)
+    ref = fp64_reference(n, row, col, val, X)
+    xt = torch.from_numpy(X).to(DEV)
+    for g in (gh, gd, go):
+        y = g.spmm(xt, schedule=S.SCHEDULE_ROWS)
+        torch.cuda.synchronize()
+        assert rel(y.cpu().numpy(), ref) <= TOL_F32
+
+
 def test_rows_item_counters_across_tile_counts(case12):
     """Work items are drawn from counters kept in the graph (one per feature
     tile) and put back to zero by the last warp of each launch: calls with 1,
