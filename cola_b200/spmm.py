@@ -104,7 +104,9 @@ class Graph:
         """Y = A X (Y += A X with accumulate).  X: (>= N) x K CUDA tensor,
         float32 or bfloat16; Y: N x K float32 or bfloat16 (allocated when None).
         unroll, min_blocks and k_tile tune the row-major schedule (0 = the
-        library's choice; every choice gives the same bits)."""
+        library's choice; every choice gives the same bits).  Calls on one
+        graph share its work-item counters and hub workspace: issue them on
+        one stream (or order the streams), not concurrently."""
         _dense(X, "X")
         K = X.shape[1]
         if X.shape[0] < self.num_nodes:
